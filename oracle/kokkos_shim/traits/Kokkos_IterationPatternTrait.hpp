@@ -1,0 +1,2 @@
+// Kokkos-compatible host shim (oracle test infrastructure): intentionally empty.
+#pragma once

@@ -1,0 +1,385 @@
+// Oracle harness over the UNMODIFIED reference solver (test infrastructure).
+//
+// Compiled against the reference's own headers (src/ of RetrO598/DGSEM) and
+// the project-written Kokkos-compatible shim in oracle/kokkos_shim.  Every
+// numerical operation executed here is the reference's code:
+//   StructuredSolver::calc_rhs          solver/structured_solver.hpp:466-480
+//   SSPRK3::step                        time_integrator/SSPRK3.hpp:159-181
+//   HGIndicator<.,.,2/3>::operator()    subcell_limiting/indicator.hpp:337,455
+//   StructuredElementInitializer        containers/data_container.hpp:729-772
+//   LobattoLegendreBasis::initialize    polynomial_basis/basis.hpp:69-153
+// The only project-written numerics are the initial/boundary state functors
+// of the benchmark cases (their formulas follow the reference examples
+// Euler2D/double_mach_reflection/double_mach_reflection_structured.cpp:9-32,
+// Euler2D/kelvin_helmholtz_hg/kelvin_helmholtz_hg.cpp IC and
+// Euler3D/inviscid_tgv/inviscid_tgv.cpp:18-35).
+//
+// Arrays cross this C ABI in the reference's logical LayoutRight order:
+//   u(i, j[, k], dof, var),  dof = local_dof(inode, jnode[, knode]).
+#include <base/base.hpp>
+#include <boundary_condition/boundary_condition.hpp>
+#include <containers/containers.hpp>
+#include <equations/equations.hpp>
+#include <mesh/mesh.hpp>
+#include <polynomial_basis/polynomial_basis.hpp>
+#include <solver/solver.hpp>
+#include <space_integral/space_integral.hpp>
+#include <subcell_limiting/subcell_limiting.hpp>
+#include <time_integrator/time_integrator.hpp>
+#include <utils/utils.hpp>
+
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <numbers>
+
+extern "C" {
+// Case kinds understood by the harness.
+enum {
+  REF_EULER2D_PERIODIC_SPLIT = 0,  // KH-like plain split form
+  REF_EULER2D_PERIODIC_HG = 1,     // periodic + HG shock capturing
+  REF_EULER2D_DMR_HG = 2,          // double Mach reflection BCs + HG
+  REF_EULER3D_PERIODIC_SPLIT = 3,  // TGV-like plain split form
+  REF_EULER3D_PERIODIC_HG = 4,     // 3D periodic + HG
+  REF_NS2D_PERIODIC_SPLIT = 5,     // Navier-Stokes BR1 + split form
+};
+
+typedef struct {
+  int kind;
+  int polydeg;
+  int n_cells[3];
+  double left[3];
+  double right[3];
+  double gamma;
+  double mu;
+  double prandtl;
+  double alpha_max;
+  double alpha_min;
+} dgsem_ref_case;
+}
+
+namespace {
+
+using T = double;
+
+// Double Mach reflection state; formula of the reference example
+// double_mach_reflection_structured.cpp:9-32.
+inline std::array<T, 4> dmr_state(const std::array<T, 2>& c, T time, T gamma) {
+  constexpr T one_sixth = static_cast<T>(1.0 / 6.0);
+  const T shock = one_sixth + (c[1] + static_cast<T>(20.0) * time) /
+                                  std::sqrt(static_cast<T>(3.0));
+  if (c[0] < shock) {
+    constexpr T phi = static_cast<T>(std::numbers::pi / 6.0);
+    const T s = std::sin(phi);
+    const T co = std::cos(phi);
+    return DGSEM::utils::prim_to_cons(
+        std::array<T, 4>{static_cast<T>(8.0), static_cast<T>(8.25) * co,
+                         -static_cast<T>(8.25) * s, static_cast<T>(116.5)},
+        gamma);
+  }
+  return DGSEM::utils::prim_to_cons(
+      std::array<T, 4>{static_cast<T>(1.4), T(0), T(0), static_cast<T>(1.0)},
+      gamma);
+}
+
+struct DmrBoundaryState {
+  T gamma;
+  std::array<T, 4> operator()(const std::array<T, 2>& c, T t) const {
+    return dmr_state(c, t, gamma);
+  }
+};
+struct DmrBottomInflow {
+  bool operator()(const std::array<T, 2>& c, T) const {
+    return c[0] < static_cast<T>(1.0 / 6.0);
+  }
+};
+
+class RefCaseBase {
+ public:
+  virtual ~RefCaseBase() = default;
+  virtual void rhs(const T* u, T* du, T t) = 0;
+  virtual void alpha(const T* u, T* a) = 0;
+  virtual void steps(T* u, T t0, T dt, int n) = 0;
+  virtual void geometry(T* coords, T* ja, T* inv_j) = 0;
+  virtual std::size_t state_size() const = 0;
+};
+
+template <class Eq, std::size_t N, class VolumeFlux, class Boundaries,
+          std::size_t D>
+class RefCase final : public RefCaseBase {
+ public:
+  using Basis = DGSEM::Basis::LobattoLegendreBasis<T, N>;
+  using Mesh = DGSEM::StructuredMesh<T, D>;
+  using Solver = DGSEM::StructuredSolver<Eq, Basis, VolumeFlux,
+                                         DGSEM::LaxFriedrichsFlux<Eq>, Mesh,
+                                         Boundaries>;
+  using Sol = DGSEM::Solution<Mesh, Basis, Eq>;
+
+  RefCase(const dgsem_ref_case& c, const Eq& eq, const Boundaries& bcs,
+          bool periodic)
+      : mesh_(make_left(c), make_right(c), make_cells(c)),
+        solver_(eq, mesh_, container_, bcs, make_periodic(periodic)),
+        sol_(mesh_),
+        c_(c) {
+    solver_.set_indicator_parameters(c.alpha_max, c.alpha_min, false);
+  }
+
+  static std::array<T, D> make_left(const dgsem_ref_case& c) {
+    std::array<T, D> a{};
+    for (std::size_t i = 0; i < D; ++i) a[i] = c.left[i];
+    return a;
+  }
+  static std::array<T, D> make_right(const dgsem_ref_case& c) {
+    std::array<T, D> a{};
+    for (std::size_t i = 0; i < D; ++i) a[i] = c.right[i];
+    return a;
+  }
+  static std::array<std::size_t, D> make_cells(const dgsem_ref_case& c) {
+    std::array<std::size_t, D> a{};
+    for (std::size_t i = 0; i < D; ++i) a[i] = c.n_cells[i];
+    return a;
+  }
+  static std::array<bool, D> make_periodic(bool p) {
+    std::array<bool, D> a{};
+    a.fill(p);
+    return a;
+  }
+
+  std::size_t state_size() const override { return sol_.u_device.size(); }
+
+  void rhs(const T* u, T* du, T t) override {
+    std::memcpy(sol_.u_device.data(), u, state_size() * sizeof(T));
+    solver_.calc_rhs(sol_, t);
+    std::memcpy(du, sol_.du_device.data(), state_size() * sizeof(T));
+  }
+
+  void alpha(const T* u, T* a) override {
+    std::memcpy(sol_.u_device.data(), u, state_size() * sizeof(T));
+    using ElementArray =
+        typename DGSEM::solution_type_traits<T, D>::ElementArray;
+    auto cells = make_cells(c_);
+    ElementArray av;
+    if constexpr (D == 2) {
+      av = ElementArray("alpha", cells[0], cells[1]);
+    } else {
+      av = ElementArray("alpha", cells[0], cells[1], cells[2]);
+    }
+    DGSEM::HGIndicator<Basis, Eq> ind(c_.alpha_max, c_.alpha_min, false,
+                                      Basis::device_data());
+    ind(cells, sol_.u_device, av);
+    std::memcpy(a, av.data(), av.size() * sizeof(T));
+  }
+
+  void steps(T* u, T t0, T dt, int n) override {
+    std::memcpy(sol_.u_device.data(), u, state_size() * sizeof(T));
+    if (!integrator_) {
+      integrator_ = std::make_unique<DGSEM::SSPRK3<T, Solver, Mesh, Sol>>(
+          sol_, mesh_, t0 + n * dt);
+    }
+    // SSPRK3::step reads the integrator's own clock; drive it through the
+    // public step() with the stage times t, t+dt, t+dt/2 of that clock.
+    for (int s = 0; s < n; ++s) {
+      StepAccess::set_time(*integrator_, t0 + s * dt);
+      integrator_->step(solver_, sol_, dt);
+    }
+    std::memcpy(u, sol_.u_device.data(), state_size() * sizeof(T));
+  }
+
+  void geometry(T* coords, T* ja, T* inv_j) override {
+    if (coords)
+      std::memcpy(coords, container_.node_coordinates.data(),
+                  container_.node_coordinates.size() * sizeof(T));
+    if (ja)
+      std::memcpy(ja, container_.contravariant_vectors.data(),
+                  container_.contravariant_vectors.size() * sizeof(T));
+    if (inv_j)
+      std::memcpy(inv_j, container_.inverse_jacobian.data(),
+                  container_.inverse_jacobian.size() * sizeof(T));
+  }
+
+ private:
+  // TimeIntegrator keeps `time` protected; a derived accessor sets it.
+  struct StepAccess : DGSEM::SSPRK3<T, Solver, Mesh, Sol> {
+    static void set_time(DGSEM::SSPRK3<T, Solver, Mesh, Sol>& ig, T t) {
+      static_cast<StepAccess&>(ig).time = t;
+    }
+  };
+
+  Mesh mesh_;
+  DGSEM::StructuredElementContainer<T, D> container_;
+  Solver solver_;
+  Sol sol_;
+  dgsem_ref_case c_;
+  std::unique_ptr<DGSEM::SSPRK3<T, Solver, Mesh, Sol>> integrator_;
+};
+
+template <std::size_t N>
+RefCaseBase* make_case_n(const dgsem_ref_case& c) {
+  using Basis = DGSEM::Basis::LobattoLegendreBasis<T, N>;
+  Basis::initialize();
+  using E2 = DGSEM::equations::CompressibleEuler2D<T>;
+  using E3 = DGSEM::equations::CompressibleEuler3D<T>;
+  using NS2 = DGSEM::equations::CompressibleNavierStokes2D<T>;
+  using P = DGSEM::PeriodicBC;
+  switch (c.kind) {
+    case REF_EULER2D_PERIODIC_SPLIT: {
+      using VF = DGSEM::VolumeIntegralSplitForm<Basis, E2, DGSEM::ChandrashekarFlux>;
+      auto b = DGSEM::BoundarySet(P{}, P{}, P{}, P{});
+      return new RefCase<E2, N, VF, decltype(b), 2>(c, E2{c.gamma}, b, true);
+    }
+    case REF_EULER2D_PERIODIC_HG: {
+      using VF = DGSEM::VolumeIntegralShockCapturingHG<
+          Basis, E2, DGSEM::ChandrashekarFlux, DGSEM::LaxFriedrichsFlux,
+          DGSEM::HGIndicator<Basis, E2>>;
+      auto b = DGSEM::BoundarySet(P{}, P{}, P{}, P{});
+      return new RefCase<E2, N, VF, decltype(b), 2>(c, E2{c.gamma}, b, true);
+    }
+    case REF_EULER2D_DMR_HG: {
+      using VF = DGSEM::VolumeIntegralShockCapturingHG<
+          Basis, E2, DGSEM::ChandrashekarFlux, DGSEM::LaxFriedrichsFlux,
+          DGSEM::HGIndicator<Basis, E2>>;
+      DmrBoundaryState inflow{c.gamma};
+      auto b = DGSEM::BoundarySet(
+          DGSEM::DirichletBC(inflow), DGSEM::OutflowBC{},
+          DGSEM::MixedDirichletSlipWallBC(inflow, DmrBottomInflow{}),
+          DGSEM::DirichletBC(inflow));
+      return new RefCase<E2, N, VF, decltype(b), 2>(c, E2{c.gamma}, b, false);
+    }
+    case REF_EULER3D_PERIODIC_SPLIT: {
+      using VF = DGSEM::VolumeIntegralSplitForm<Basis, E3, DGSEM::ChandrashekarFlux>;
+      auto b = DGSEM::BoundarySet(P{}, P{}, P{}, P{}, P{}, P{});
+      return new RefCase<E3, N, VF, decltype(b), 3>(c, E3{c.gamma}, b, true);
+    }
+    case REF_EULER3D_PERIODIC_HG: {
+      using VF = DGSEM::VolumeIntegralShockCapturingHG<
+          Basis, E3, DGSEM::ChandrashekarFlux, DGSEM::LaxFriedrichsFlux,
+          DGSEM::HGIndicator<Basis, E3>>;
+      auto b = DGSEM::BoundarySet(P{}, P{}, P{}, P{}, P{}, P{});
+      return new RefCase<E3, N, VF, decltype(b), 3>(c, E3{c.gamma}, b, true);
+    }
+    case REF_NS2D_PERIODIC_SPLIT: {
+      using VF = DGSEM::VolumeIntegralSplitForm<Basis, NS2, DGSEM::ChandrashekarFlux>;
+      auto b = DGSEM::BoundarySet(P{}, P{}, P{}, P{});
+      return new RefCase<NS2, N, VF, decltype(b), 2>(
+          c, NS2{c.gamma, c.mu, c.prandtl}, b, true);
+    }
+    default:
+      return nullptr;
+  }
+}
+
+RefCaseBase* make_case(const dgsem_ref_case& c) {
+  const bool is3d = c.kind == REF_EULER3D_PERIODIC_SPLIT ||
+                    c.kind == REF_EULER3D_PERIODIC_HG;
+  if (is3d) {
+    switch (c.polydeg) {
+      case 1: return make_case_n<1>(c);
+      case 2: return make_case_n<2>(c);
+      case 3: return make_case_n<3>(c);
+      case 4: return make_case_n<4>(c);
+      default: return nullptr;
+    }
+  }
+  switch (c.polydeg) {
+    case 1: return make_case_n<1>(c);
+    case 2: return make_case_n<2>(c);
+    case 3: return make_case_n<3>(c);
+    case 4: return make_case_n<4>(c);
+    case 5: return make_case_n<5>(c);
+    case 6: return make_case_n<6>(c);
+    case 7: return make_case_n<7>(c);
+    default: return nullptr;
+  }
+}
+
+template <std::size_t N>
+void basis_tables_n(double* out) {
+  using Basis = DGSEM::Basis::LobattoLegendreBasis<T, N>;
+  Basis::initialize();
+  constexpr std::size_t n = N + 1;
+  auto d = Basis::device_data();
+  std::size_t o = 0;
+  for (std::size_t i = 0; i < n; ++i) out[o++] = d.nodes(i);
+  for (std::size_t i = 0; i < n; ++i) out[o++] = d.weights(i);
+  for (std::size_t i = 0; i < n; ++i) out[o++] = d.inv_weights(i);
+  for (std::size_t i = 0; i < n; ++i) out[o++] = d.boundary_interpolation_left(i);
+  for (std::size_t i = 0; i < n; ++i) out[o++] = d.boundary_interpolation_right(i);
+  for (std::size_t i = 0; i < n; ++i)
+    for (std::size_t j = 0; j < n; ++j) out[o++] = d.derivative_matrix(i, j);
+  for (std::size_t i = 0; i < n; ++i)
+    for (std::size_t j = 0; j < n; ++j) out[o++] = d.derivative_split(i, j);
+  for (std::size_t i = 0; i < n; ++i)
+    for (std::size_t j = 0; j < n; ++j) out[o++] = d.derivative_dhat(i, j);
+  for (std::size_t i = 0; i < n; ++i)
+    for (std::size_t j = 0; j < n; ++j)
+      out[o++] = d.inverse_vandermonde_legendre(i, j);
+}
+
+}  // namespace
+
+extern "C" {
+
+void* dgsem_ref_create(const dgsem_ref_case* c) {
+  if (!c) return nullptr;
+  if (!Kokkos::is_initialized()) Kokkos::initialize();
+  return make_case(*c);
+}
+
+void dgsem_ref_destroy(void* h) { delete static_cast<RefCaseBase*>(h); }
+
+long long dgsem_ref_state_size(void* h) {
+  return h ? static_cast<long long>(static_cast<RefCaseBase*>(h)->state_size())
+           : -1;
+}
+
+int dgsem_ref_rhs(void* h, const double* u, double* du, double t) {
+  if (!h) return -1;
+  static_cast<RefCaseBase*>(h)->rhs(u, du, t);
+  return 0;
+}
+
+int dgsem_ref_alpha(void* h, const double* u, double* alpha) {
+  if (!h) return -1;
+  static_cast<RefCaseBase*>(h)->alpha(u, alpha);
+  return 0;
+}
+
+int dgsem_ref_ssprk3(void* h, double* u, double t0, double dt, int nsteps) {
+  if (!h) return -1;
+  static_cast<RefCaseBase*>(h)->steps(u, t0, dt, nsteps);
+  return 0;
+}
+
+int dgsem_ref_geometry(void* h, double* coords, double* ja, double* inv_j) {
+  if (!h) return -1;
+  static_cast<RefCaseBase*>(h)->geometry(coords, ja, inv_j);
+  return 0;
+}
+
+// Basis tables in the order nodes, weights, inv_weights, lhat(-1), lhat(+1),
+// D, Dsplit, Dhat, inverse Legendre Vandermonde (row-major n x n each).
+int dgsem_ref_basis(int polydeg, double* out) {
+  if (!Kokkos::is_initialized()) Kokkos::initialize();
+  switch (polydeg) {
+    case 1: basis_tables_n<1>(out); return 0;
+    case 2: basis_tables_n<2>(out); return 0;
+    case 3: basis_tables_n<3>(out); return 0;
+    case 4: basis_tables_n<4>(out); return 0;
+    case 5: basis_tables_n<5>(out); return 0;
+    case 6: basis_tables_n<6>(out); return 0;
+    case 7: basis_tables_n<7>(out); return 0;
+    default: return -1;
+  }
+}
+
+int dgsem_ref_omp_threads(void) {
+#ifdef _OPENMP
+  extern int omp_get_max_threads(void);
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+}  // extern "C"
