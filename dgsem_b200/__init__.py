@@ -1,0 +1,16 @@
+"""dgsem_b200: B200-native (sm_100a) FP64 DGSEM right-hand side and fused
+SSPRK3 stage update, with the reference solver's plugin surface.
+
+The compute path is libdgsem_b200.so (hand-written CUDA kernels behind the C
+ABI in include/dgsem_b200.h); this package is its host-side mirror.
+"""
+from ._capi import DgsemError, lib  # noqa: F401
+from .solver import (  # noqa: F401
+    BoundarySet, ChandrashekarFlux, CompressibleEuler2D, CompressibleEuler3D,
+    CompressibleNavierStokes2D, DirichletBC, DoubleMachReflectionInitial, HGIndicator,
+    HLLCFlux, InviscidTaylorGreenVortex, IsentropicVortex, KelvinHelmholtzInitial,
+    KennedyGruberFlux, LaxFriedrichsFlux, LobattoLegendreBasis,
+    MixedDirichletSlipWallBC, OutflowBC, PeriodicBC, RanochaFlux, SlipWallBC, Solution,
+    SSPRK3, StructuredMesh, StructuredSolver, TaylorGreenVortex2D,
+    VolumeIntegralShockCapturingHG, VolumeIntegralSplitForm,
+)

@@ -1,0 +1,128 @@
+// Type-erased solver engine: one instantiation per supported template
+// combination (dimension, nodes per direction, volume flux, surface flux,
+// shock capturing).  The C ABI context owns one engine.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <memory>
+
+#include "stage_kernel.cuh"
+#include "tables.hpp"
+
+namespace dgsem {
+
+// Everything an engine needs that does not depend on its template arguments.
+struct EngineConfig {
+  int ndims;
+  int n;
+  int64_t cells[3];
+  int periodic[3];
+  int64_t nelem;
+  double gamma;
+  double mu, prandtl;
+  double alpha_max, alpha_min, atol;
+  double hg_threshold, hg_s;
+  DeviceTables tab;
+  BcParams bc;
+  BasisTables basis;
+  unsigned int* nonfinite;  // device flag
+};
+
+class EngineBase {
+ public:
+  virtual ~EngineBase() = default;
+  // out = a*u_n + b*u_in + c*RHS(u_in, t); alpha_out optional.
+  virtual cudaError_t stage(const EngineConfig& cfg, const double* u_n,
+                            const double* u_in, double* out, double a, double b,
+                            double c, double t, double* alpha_out,
+                            cudaStream_t s) = 0;
+  virtual int elements_per_block() const = 0;
+  virtual int threads_per_block() const = 0;
+  virtual size_t smem_bytes() const = 0;
+};
+
+std::unique_ptr<EngineBase> make_engine(int ndims, int n, int vf, int sf,
+                                        bool hg);
+
+template <int N>
+inline void fill_basis_const(const BasisTables& b, BasisConst<N>* out) {
+  for (int i = 0; i < N; ++i) {
+    for (int j = 0; j < N; ++j) {
+      out->Dsplit[i][j] = b.Dsplit[i][j];
+      out->Dhat[i][j] = b.Dhat[i][j];
+      out->Vinv[i][j] = b.Vinv[i][j];
+    }
+    out->inv_w[i] = b.inv_weights[i];
+  }
+  out->lhat_l0 = b.lhat_left[0];
+  out->lhat_rN = b.lhat_right[N - 1];
+}
+
+// Launch geometry per (DIM, N): one thread per element line.
+template <int DIM, int N>
+struct LaunchShape {
+  static constexpr int NLINE = DIM * ipow(N, DIM - 1);
+  static constexpr int TARGET = DIM == 2 ? 128 : 96;
+  static constexpr int EPB = (TARGET / NLINE) > 0 ? (TARGET / NLINE) : 1;
+  static constexpr int NT = ((EPB * NLINE + 31) / 32) * 32;
+};
+
+template <int DIM, int N, int VF, int SF, bool HG>
+class Engine final : public EngineBase {
+ public:
+  using L = LaunchShape<DIM, N>;
+  static constexpr int EPB = L::EPB;
+  static constexpr int NT = L::NT;
+  using Shape = StageShape<DIM, N, VF, SF, HG, EPB>;
+
+  Engine() {
+    cudaFuncSetAttribute(stage_kernel<DIM, N, VF, SF, HG, EPB, NT>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)Shape::smem_bytes);
+  }
+
+  cudaError_t stage(const EngineConfig& cfg, const double* u_n,
+                    const double* u_in, double* out, double a, double b,
+                    double c, double t, double* alpha_out,
+                    cudaStream_t s) override {
+    StageArgs<N> args;
+    args.u_in = u_in;
+    args.u_n = u_n;
+    args.out = out;
+    args.a = a;
+    args.b = b;
+    args.c = c;
+    args.t = t;
+    for (int i = 0; i < 3; ++i) {
+      args.cells[i] = cfg.cells[i];
+      args.periodic[i] = cfg.periodic[i];
+    }
+    args.nelem = cfg.nelem;
+    args.gamma = cfg.gamma;
+    args.inv_gm1 = 1.0 / (cfg.gamma - 1.0);
+    args.alpha_max = cfg.alpha_max;
+    args.alpha_min = cfg.alpha_min;
+    args.atol = cfg.atol;
+    args.hg_threshold = cfg.hg_threshold;
+    args.hg_s = cfg.hg_s;
+    args.alpha_out = alpha_out;
+    args.nonfinite = cfg.nonfinite;
+    args.grad = nullptr;
+    args.mu = cfg.mu;
+    args.kappa = cfg.gamma / ((cfg.gamma - 1.0) * cfg.prandtl);
+    args.tab = cfg.tab;
+    args.bc = cfg.bc;
+    fill_basis_const<N>(cfg.basis, &args.basis);
+    const int64_t blocks = (cfg.nelem + EPB - 1) / EPB;
+    stage_kernel<DIM, N, VF, SF, HG, EPB, NT>
+        <<<(unsigned)blocks, NT, Shape::smem_bytes, s>>>(args);
+    return cudaGetLastError();
+  }
+  int elements_per_block() const override { return EPB; }
+  int threads_per_block() const override { return NT; }
+  size_t smem_bytes() const override { return Shape::smem_bytes; }
+};
+
+}  // namespace dgsem

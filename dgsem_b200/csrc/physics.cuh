@@ -1,0 +1,295 @@
+// Device physics for the compressible Euler / Navier-Stokes DGSEM right-hand
+// side: logarithmic mean, two-point volume fluxes and surface fluxes.
+//
+// Every flux works on per-node primitive data prepared once per node
+// (`NodeState`), so the per-pair cost is only the two-point averages.  The
+// formulas follow the reference's plugins:
+//   ln_mean                      base/math_utils.hpp:8-25
+//   ChandrashekarFlux 2D/3D      base/numerical_flux.hpp:436-500, 520-594
+//   LaxFriedrichsFlux 2D/3D      base/numerical_flux.hpp:198-228, 39-69
+//   LLF wave speed |v.n|+a|n|    equations/compressible_euler2D.hpp:70-109
+//   HLLC (1D, Roe/Einfeldt)      base/numerical_flux.hpp:283-378
+// and, for fluxes the reference does not ship, the published formulas:
+//   Ranocha (J. Sci. Comput. 2018 / 2020), Kennedy & Gruber (JCP 2008).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace dgsem {
+
+enum VolumeFluxKind : int { VF_CHANDRASHEKAR = 0, VF_RANOCHA = 1, VF_KENNEDY_GRUBER = 2 };
+enum SurfaceFluxKind : int { SF_LLF = 0, SF_HLLC = 1 };
+
+// Per-node data shared by all two-point fluxes (SoA in shared memory).
+template <int DIM>
+struct NodeState {
+  double rho;
+  double v[DIM];
+  double p;
+  double beta;  // 0.5 rho / p  (Chandrashekar); e = E / rho (Kennedy-Gruber)
+  double kin;   // 0.5 |v|^2
+};
+
+// Logarithmic mean and its inverse with the reference's branch rule
+// (series when f^2 < 1e-4, else (y-x)/log(y/x)).  The series branch reuses one
+// reciprocal of x+y for f^2 and for the inverse mean.
+__device__ __forceinline__ void ln_mean_parts(double x, double y, double& mean,
+                                              double& inv_mean) {
+  const double s = x + y;
+  const double r = 1.0 / s;
+  const double t = (x - y) * r;
+  const double f2 = t * t;
+  if (f2 < 1.0e-4) {
+    const double poly =
+        2.0 + f2 * (2.0 / 3.0 + f2 * (2.0 / 5.0 + f2 * (2.0 / 7.0)));
+    mean = s / poly;
+    inv_mean = poly * r;
+  } else {
+    const double lg = log(y / x);
+    mean = (y - x) / lg;
+    inv_mean = lg / (y - x);
+  }
+}
+
+__device__ __forceinline__ double ln_mean(double x, double y) {
+  const double s = x + y;
+  const double t = (x - y) / s;
+  const double f2 = t * t;
+  if (f2 < 1.0e-4) {
+    const double poly =
+        2.0 + f2 * (2.0 / 3.0 + f2 * (2.0 / 5.0 + f2 * (2.0 / 7.0)));
+    return s / poly;
+  }
+  return (y - x) / log(y / x);
+}
+
+__device__ __forceinline__ double inv_ln_mean(double x, double y) {
+  const double s = x + y;
+  const double r = 1.0 / s;
+  const double t = (x - y) * r;
+  const double f2 = t * t;
+  if (f2 < 1.0e-4) {
+    const double poly =
+        2.0 + f2 * (2.0 / 3.0 + f2 * (2.0 / 5.0 + f2 * (2.0 / 7.0)));
+    return poly * r;
+  }
+  return log(y / x) / (y - x);
+}
+
+// Node preparation from conserved variables (rho, m_1..m_DIM, E).
+template <int DIM, int VF>
+__device__ __forceinline__ NodeState<DIM> prepare_node(const double* u,
+                                                       double gamma) {
+  NodeState<DIM> s;
+  s.rho = u[0];
+  const double inv_rho = 1.0 / u[0];
+  double sq = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    s.v[d] = u[1 + d] * inv_rho;
+    sq += s.v[d] * s.v[d];
+  }
+  s.kin = 0.5 * sq;
+  s.p = (gamma - 1.0) * (u[DIM + 1] - 0.5 * u[0] * sq);
+  if (VF == VF_KENNEDY_GRUBER) {
+    s.beta = u[DIM + 1] * inv_rho;
+  } else {
+    s.beta = 0.5 * u[0] / s.p;
+  }
+  return s;
+}
+
+// Two-point volume flux f(L, R; normal) -> f[DIM + 2].
+template <int DIM, int VF>
+__device__ __forceinline__ void volume_flux(const NodeState<DIM>& L,
+                                            const NodeState<DIM>& R,
+                                            const double* n, double inv_gm1,
+                                            double* f) {
+  double vnL = 0.0, vnR = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    vnL += L.v[d] * n[d];
+    vnR += R.v[d] * n[d];
+  }
+  if (VF == VF_CHANDRASHEKAR) {
+    // numerical_flux.hpp:436-500: rho_mean = ln(rho), beta_mean = ln(beta),
+    // p_mean = 0.5 rho_avg / beta_avg = 0.5 (rhoL+rhoR) / (betaL+betaR).
+    double rho_mean, unused;
+    ln_mean_parts(L.rho, R.rho, rho_mean, unused);
+    double beta_mean_unused, inv_beta_mean;
+    ln_mean_parts(L.beta, R.beta, beta_mean_unused, inv_beta_mean);
+    const double p_mean = 0.5 * (L.rho + R.rho) / (L.beta + R.beta);
+    const double f1 = rho_mean * 0.5 * (vnL + vnR);
+    f[0] = f1;
+    double fe = f1 * 0.5 * (inv_gm1 * inv_beta_mean - (L.kin + R.kin));
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      const double va = 0.5 * (L.v[d] + R.v[d]);
+      const double fm = f1 * va + p_mean * n[d];
+      f[1 + d] = fm;
+      fe += fm * va;
+    }
+    f[DIM + 1] = fe;
+  } else if (VF == VF_RANOCHA) {
+    const double rho_mean = ln_mean(L.rho, R.rho);
+    const double inv_rho_p_mean =
+        L.p * R.p * inv_ln_mean(L.rho * R.p, R.rho * L.p);
+    const double p_avg = 0.5 * (L.p + R.p);
+    double vLvR = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) vLvR += L.v[d] * R.v[d];
+    const double f1 = rho_mean * 0.5 * (vnL + vnR);
+    f[0] = f1;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d)
+      f[1 + d] = f1 * (0.5 * (L.v[d] + R.v[d])) + p_avg * n[d];
+    f[DIM + 1] = f1 * (0.5 * vLvR + inv_rho_p_mean * inv_gm1) +
+                 0.5 * (L.p * vnR + R.p * vnL);
+  } else {  // Kennedy-Gruber
+    const double rho_avg = 0.5 * (L.rho + R.rho);
+    const double e_avg = 0.5 * (L.beta + R.beta);
+    const double p_avg = 0.5 * (L.p + R.p);
+    double vn_avg = 0.0;
+    double va[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      va[d] = 0.5 * (L.v[d] + R.v[d]);
+      vn_avg += va[d] * n[d];
+    }
+    const double f1 = rho_avg * vn_avg;
+    f[0] = f1;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) f[1 + d] = f1 * va[d] + p_avg * n[d];
+    f[DIM + 1] = (rho_avg * e_avg + p_avg) * vn_avg;
+  }
+}
+
+// Primitive data used by the surface fluxes.
+template <int DIM>
+struct FaceState {
+  double u[DIM + 2];
+  double v[DIM];
+  double p;
+  double a;  // sound speed
+};
+
+template <int DIM>
+__device__ __forceinline__ FaceState<DIM> prepare_face(const double* u,
+                                                       double gamma) {
+  FaceState<DIM> s;
+#pragma unroll
+  for (int q = 0; q < DIM + 2; ++q) s.u[q] = u[q];
+  const double inv_rho = 1.0 / u[0];
+  double sq = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    s.v[d] = u[1 + d] * inv_rho;
+    sq += s.v[d] * s.v[d];
+  }
+  s.p = (gamma - 1.0) * (u[DIM + 1] - 0.5 * u[0] * sq);
+  s.a = sqrt(gamma * s.p * inv_rho);
+  return s;
+}
+
+// Local Lax-Friedrichs flux (numerical_flux.hpp:198-228 with the wave speed
+// of compressible_euler2D.hpp:70-109): 0.5 (F_L + F_R).n - 0.5 lambda (uR-uL).
+template <int DIM>
+__device__ __forceinline__ void llf_flux(const FaceState<DIM>& L,
+                                         const FaceState<DIM>& R,
+                                         const double* n, double* f) {
+  double vnL = 0.0, vnR = 0.0, nn = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    vnL += L.v[d] * n[d];
+    vnR += R.v[d] * n[d];
+    nn += n[d] * n[d];
+  }
+  const double lam =
+      fmax(fabs(vnL), fabs(vnR)) + fmax(L.a, R.a) * sqrt(nn);
+  f[0] = 0.5 * (L.u[0] * vnL + R.u[0] * vnR) - 0.5 * lam * (R.u[0] - L.u[0]);
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    const double fl = L.u[1 + d] * vnL + L.p * n[d];
+    const double fr = R.u[1 + d] * vnR + R.p * n[d];
+    f[1 + d] = 0.5 * (fl + fr) - 0.5 * lam * (R.u[1 + d] - L.u[1 + d]);
+  }
+  f[DIM + 1] = 0.5 * (vnL * (L.u[DIM + 1] + L.p) + vnR * (R.u[DIM + 1] + R.p)) -
+               0.5 * lam * (R.u[DIM + 1] - L.u[DIM + 1]);
+}
+
+// Normal-rotated HLLC for 2D Euler: the reference's 1D HLLC
+// (numerical_flux.hpp:283-378) in the face frame, tangential momentum carried
+// passively, rotated back and scaled by |n|.
+__device__ __forceinline__ void hllc_flux_2d(const FaceState<2>& Ls,
+                                             const FaceState<2>& Rs,
+                                             const double* n, double gamma,
+                                             double* f) {
+  const double nn = sqrt(n[0] * n[0] + n[1] * n[1]);
+  const double nx = n[0] / nn, ny = n[1] / nn;
+  const double rL = Ls.u[0], rR = Rs.u[0];
+  const double mnL = Ls.u[1] * nx + Ls.u[2] * ny;
+  const double mtL = -Ls.u[1] * ny + Ls.u[2] * nx;
+  const double mnR = Rs.u[1] * nx + Rs.u[2] * ny;
+  const double mtR = -Rs.u[1] * ny + Rs.u[2] * nx;
+  const double EL = Ls.u[3], ER = Rs.u[3];
+  const double vL = mnL / rL, vR = mnR / rR;
+  const double wL = mtL / rL, wR = mtR / rR;
+  const double pL = (gamma - 1.0) * (EL - 0.5 * rL * (vL * vL + wL * wL));
+  const double pR = (gamma - 1.0) * (ER - 0.5 * rR * (vR * vR + wR * wR));
+  const double cL = sqrt(gamma * pL / rL);
+  const double cR = sqrt(gamma * pR / rR);
+  const double srL = sqrt(rL), srR = sqrt(rR);
+  const double ssum = srL + srR;
+  const double v_roe = (srL * vL + srR * vR) / ssum;
+  const double w_roe = (srL * wL + srR * wR) / ssum;
+  const double ekin_roe = 0.5 * (v_roe * v_roe + w_roe * w_roe);
+  const double HL = (EL + pL) / rL;
+  const double HR = (ER + pR) / rR;
+  const double H_roe = (srL * HL + srR * HR) / ssum;
+  const double c_roe = sqrt((gamma - 1.0) * (H_roe - ekin_roe));
+  const double SL = fmin(vL - cL, v_roe - c_roe);
+  const double SR = fmax(vR + cR, v_roe + c_roe);
+  double g[4];
+  if (SL >= 0.0) {
+    g[0] = mnL; g[1] = mnL * vL + pL; g[2] = mnL * wL; g[3] = vL * (EL + pL);
+  } else if (SR <= 0.0) {
+    g[0] = mnR; g[1] = mnR * vR + pR; g[2] = mnR * wR; g[3] = vR * (ER + pR);
+  } else {
+    const double sMuL = SL - vL, sMuR = SR - vR;
+    const double SStar = (pR - pL + rL * vL * sMuL - rR * vR * sMuR) /
+                         (rL * sMuL - rR * sMuR);
+    if (SStar >= 0.0) {
+      const double dS = rL * sMuL / (SL - SStar);
+      const double eS = EL / rL + (SStar - vL) * (SStar + pL / (rL * sMuL));
+      g[0] = mnL + SL * (dS - rL);
+      g[1] = (mnL * vL + pL) + SL * (dS * SStar - mnL);
+      g[2] = mnL * wL + SL * (dS * wL - mtL);
+      g[3] = vL * (EL + pL) + SL * (dS * eS - EL);
+    } else {
+      const double dS = rR * sMuR / (SR - SStar);
+      const double eS = ER / rR + (SStar - vR) * (SStar + pR / (rR * sMuR));
+      g[0] = mnR + SR * (dS - rR);
+      g[1] = (mnR * vR + pR) + SR * (dS * SStar - mnR);
+      g[2] = mnR * wR + SR * (dS * wR - mtR);
+      g[3] = vR * (ER + pR) + SR * (dS * eS - ER);
+    }
+  }
+  f[0] = g[0] * nn;
+  f[1] = (g[1] * nx - g[2] * ny) * nn;
+  f[2] = (g[1] * ny + g[2] * nx) * nn;
+  f[3] = g[3] * nn;
+}
+
+template <int DIM, int SF>
+__device__ __forceinline__ void surface_flux(const FaceState<DIM>& L,
+                                             const FaceState<DIM>& R,
+                                             const double* n, double gamma,
+                                             double* f) {
+  if constexpr (SF == SF_HLLC && DIM == 2) {
+    hllc_flux_2d(L, R, n, gamma, f);
+  } else {
+    llf_flux<DIM>(L, R, n, f);
+  }
+}
+
+}  // namespace dgsem

@@ -1,0 +1,566 @@
+// Fused DGSEM stage kernel for sm_100a: one launch computes, per element,
+//   RHS(u_in) = -1/J [ sum_dir V_dir(u_in) + surface lift ]
+// and writes either du or the SSPRK3 stage value a*u_n + b*u_in + c*du.
+//
+// Per block: EPB elements, NT threads.  Phases (shared-memory staged):
+//   0  coalesced load of the block's contiguous u_in tile  [EPB][NV][ND]
+//   1  per-node primitives (v, p, beta, kin) and, with shock capturing, the
+//      Hennemann-Gassner alpha of each element
+//   2  (a) every face node of the element's 2*DIM faces: interface or
+//          boundary flux f*, the neighbour's trace read from L2;
+//      (b) every line of the element (DIM * n^(DIM-1) of them): symmetric
+//          split-form pair loop (each two-point flux evaluated once, both
+//          endpoints accumulated in registers) plus, for troubled elements,
+//          the FV subcell fluxes along the line and the alpha blend
+//   3  sum of directions + lifting, times -1/J, SSPRK3 combination, store.
+// Reference path replaced (one Kokkos kernel per item, :line):
+//   deep_copy(du, 0)                         solver/structured_solver.hpp:469
+//   HGIndicator2D                            subcell_limiting/indicator.hpp:337-418
+//   VolumeIntegralSplit / FinitVolumeIntegral space_integral/volume_flux.hpp:221-511
+//   VolumeIntegralShockCapturingHG blend     space_integral/volume_flux.hpp:817-842
+//   InterfaceHelper::interface_flux          space_integral/surface_flux.hpp:45-271
+//   BC_Apply (Dirichlet/Outflow/Mixed)       boundary_condition/*.hpp
+//   SurfaceIntegral::integral                space_integral/surface_integral.hpp:35-154
+//   JacobianProjFunctor                      space_integral/jacobian.hpp:76-101
+//   parallel_ma2 / parallel_ma3              time_integrator/SSPRK3.hpp:12-143
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "physics.cuh"
+
+namespace dgsem {
+
+constexpr int ipow(int b, int e) { return e == 0 ? 1 : b * ipow(b, e - 1); }
+
+template <int N>
+struct BasisConst {
+  double Dsplit[N][N];
+  double Dhat[N][N];
+  double Vinv[N][N];
+  double inv_w[N];
+  double lhat_l0;  // l_0(-1) / w_0
+  double lhat_rN;  // l_N(+1) / w_N
+};
+
+struct DeviceTables {
+  const double* ja[3][3];  // ja[a][c]: [eidx_c][node]
+  const double* jdiag[3];  // [e_a * n + i]
+  const double* coord[3];  // [e_a * n + i]
+  const double* fv[2][2];  // 2D FV subcell normals [eidx_c][f * n + line]
+};
+
+enum BcKind : int {
+  BC_PERIODIC = 0,
+  BC_DIRICHLET_DMR = 1,
+  BC_OUTFLOW = 2,
+  BC_MIXED_DMR_WALL = 3,
+  BC_DIRICHLET_CONST = 4,
+  BC_SLIP_WALL = 5
+};
+
+struct BcParams {
+  int kind[6];
+  double state[4];     // DIRICHLET_CONST conserved state
+  double dmr_post[4];  // conserved post-shock state
+  double dmr_pre[4];   // conserved pre-shock state
+  double sqrt3;
+};
+
+template <int N>
+struct StageArgs {
+  const double* u_in;
+  const double* u_n;
+  double* out;
+  double a, b, c;  // out = a*u_n + b*u_in + c*du
+  double t;
+  int64_t cells[3];
+  int64_t nelem;
+  int periodic[3];
+  double gamma, inv_gm1;
+  double alpha_max, alpha_min, atol, hg_threshold, hg_s;
+  double* alpha_out;  // optional per-element alpha
+  unsigned int* nonfinite;
+  const double* grad;  // Navier-Stokes lifted gradient [E][4][2][ND]
+  double mu, kappa;
+  DeviceTables tab;
+  BcParams bc;
+  BasisConst<N> basis;
+};
+
+// ---------------------------------------------------------------------------
+// Element / node index helpers
+// ---------------------------------------------------------------------------
+
+template <int DIM>
+struct ElemIdx {
+  int64_t i[3];
+};
+
+template <int DIM>
+__device__ __forceinline__ ElemIdx<DIM> elem_coords(int64_t e, const int64_t* cells) {
+  ElemIdx<DIM> r;
+  r.i[0] = e % cells[0];
+  if (DIM == 2) {
+    r.i[1] = e / cells[0];
+    r.i[2] = 0;
+  } else {
+    r.i[1] = (e / cells[0]) % cells[1];
+    r.i[2] = e / (cells[0] * cells[1]);
+  }
+  return r;
+}
+
+// Element index over the axes other than c (tables.hpp other_axes_count).
+template <int DIM>
+__device__ __forceinline__ int64_t eidx_other(const ElemIdx<DIM>& ei, int c,
+                                              const int64_t* cells) {
+  if (DIM == 2) return c == 0 ? ei.i[1] : ei.i[0];
+  if (c == 0) return ei.i[1] + cells[1] * ei.i[2];
+  if (c == 1) return ei.i[0] + cells[0] * ei.i[2];
+  return ei.i[0] + cells[0] * ei.i[1];
+}
+
+template <int DIM>
+__device__ __forceinline__ int64_t elem_linear(const ElemIdx<DIM>& ei, const int64_t* cells) {
+  if (DIM == 2) return ei.i[0] + cells[0] * ei.i[1];
+  return ei.i[0] + cells[0] * (ei.i[1] + cells[1] * ei.i[2]);
+}
+
+// Node index of position m along line `line` in direction dir.
+template <int DIM, int N>
+__device__ __forceinline__ int line_node(int dir, int line, int m) {
+  if (DIM == 2) return dir == 0 ? m + N * line : line + N * m;
+  if (dir == 0) return m + N * line;
+  if (dir == 1) return (line % N) + N * m + N * N * (line / N);
+  return line + N * N * m;
+}
+
+// Node index of face node fn on the face of direction dir at position pos.
+template <int DIM, int N>
+__device__ __forceinline__ int face_node(int dir, int fn, int pos) {
+  return line_node<DIM, N>(dir, fn, pos);
+}
+
+__device__ __forceinline__ double ja_at(const double* tab, int64_t eidx, int nd,
+                                        int node) {
+  return __ldg(tab + eidx * nd + node);
+}
+
+// ---------------------------------------------------------------------------
+// Double Mach reflection state (examples/Euler2D/double_mach_reflection/
+// double_mach_reflection_structured.cpp:9-32); the shock position is
+// evaluated without contraction so the pre/post decision matches the
+// reference's host arithmetic.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void dmr_state(const BcParams& bc, double x, double y,
+                                          double t, double* u) {
+  const double shock = __dadd_rn(
+      1.0 / 6.0, __ddiv_rn(__dadd_rn(y, __dmul_rn(20.0, t)), bc.sqrt3));
+  const double* s = (x < shock) ? bc.dmr_post : bc.dmr_pre;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) u[q] = s[q];
+}
+
+// MixedDirichletSlipWallBC::reflect_state (dirichlet_boundary.hpp:207-220).
+__device__ __forceinline__ void reflect_state(const double* ui, const double* n,
+                                              double* uw) {
+  const double rho = ui[0];
+  const double vx = ui[1] / rho;
+  const double vy = ui[2] / rho;
+  const double nn2 = n[0] * n[0] + n[1] * n[1];
+  const double vn = (vx * n[0] + vy * n[1]) / nn2;
+  uw[0] = rho;
+  uw[1] = rho * (vx - 2.0 * vn * n[0]);
+  uw[2] = rho * (vy - 2.0 * vn * n[1]);
+  uw[3] = ui[3];
+}
+
+// ---------------------------------------------------------------------------
+// Hennemann-Gassner indicator for one element (indicator.hpp:337-418, 2D).
+// Evaluated with explicitly rounded products and sums (no contraction) in
+// the reference's order, so alpha and the troubled-cell flag match.
+// ---------------------------------------------------------------------------
+template <int N>
+__device__ double hg_alpha_2d(const double* us_el, int ND, const BasisConst<N>& B,
+                              double threshold, double s, double alpha_min,
+                              double alpha_max) {
+  double ind[N][N];
+#pragma unroll
+  for (int j = 0; j < N; ++j)
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      const int node = j * N + i;
+      const double rho = us_el[0 * ND + node];
+      const double u_vel = __ddiv_rn(us_el[1 * ND + node], rho);
+      const double v_vel = __ddiv_rn(us_el[2 * ND + node], rho);
+      const double vv = __dadd_rn(__dmul_rn(u_vel, u_vel), __dmul_rn(v_vel, v_vel));
+      const double p = __dmul_rn(1.4 - 1.0, __dsub_rn(us_el[3 * ND + node],
+                                                       __dmul_rn(__dmul_rn(0.5, rho), vv)));
+      ind[j][i] = __dmul_rn(p, rho);
+    }
+  double tmp[N][N];
+#pragma unroll
+  for (int j = 0; j < N; ++j)
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      double r = 0.0;
+#pragma unroll
+      for (int ii = 0; ii < N; ++ii) r = __dadd_rn(r, __dmul_rn(B.Vinv[i][ii], ind[j][ii]));
+      tmp[j][i] = r;
+    }
+  double total = 0.0, c1 = 0.0, c2 = 0.0;
+  double m2[N][N];
+#pragma unroll
+  for (int j = 0; j < N; ++j)
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      double r = 0.0;
+#pragma unroll
+      for (int jj = 0; jj < N; ++jj) r = __dadd_rn(r, __dmul_rn(B.Vinv[j][jj], tmp[jj][i]));
+      m2[j][i] = __dmul_rn(r, r);
+    }
+#pragma unroll
+  for (int j = 0; j < N; ++j)
+#pragma unroll
+    for (int i = 0; i < N; ++i) total = __dadd_rn(total, m2[j][i]);
+#pragma unroll
+  for (int j = 0; j + 1 < N; ++j)
+#pragma unroll
+    for (int i = 0; i + 1 < N; ++i) c1 = __dadd_rn(c1, m2[j][i]);
+#pragma unroll
+  for (int j = 0; j + 2 < N; ++j)
+#pragma unroll
+    for (int i = 0; i + 2 < N; ++i) c2 = __dadd_rn(c2, m2[j][i]);
+  const double e1 = (total != 0.0) ? __ddiv_rn(__dsub_rn(total, c1), total) : 0.0;
+  const double e2 = (c1 != 0.0) ? __ddiv_rn(__dsub_rn(c1, c2), c1) : 0.0;
+  const double energy = fmax(e1, e2);
+  double alpha = __ddiv_rn(
+      1.0, __dadd_rn(1.0, exp(__dmul_rn(__ddiv_rn(-s, threshold),
+                                        __dsub_rn(energy, threshold)))));
+  if (alpha < alpha_min) alpha = 0.0;
+  if (alpha > 1.0 - alpha_min) alpha = 1.0;
+  return fmin(alpha_max, alpha);
+}
+
+// ---------------------------------------------------------------------------
+// The fused stage kernel
+// ---------------------------------------------------------------------------
+template <int DIM, int N, int VF, int SF, bool HG, int EPB>
+struct StageShape {
+  static constexpr int NV = DIM + 2;
+  static constexpr int ND = ipow(N, DIM);
+  static constexpr int NF = ipow(N, DIM - 1);
+  static constexpr int NFACE = 2 * DIM;
+  static constexpr int NLINE = DIM * NF;
+  static constexpr int NQ = DIM + 3;  // v[DIM], p, beta, kin
+  static constexpr int SM_U = EPB * NV * ND;
+  static constexpr int SM_P = EPB * NQ * ND;
+  static constexpr int SM_F = EPB * NFACE * NV * NF;
+  static constexpr int SM_V = EPB * DIM * NV * ND;
+  static constexpr int SM_A = EPB;
+  static constexpr size_t smem_bytes =
+      sizeof(double) * (SM_U + SM_P + SM_F + SM_V + SM_A);
+};
+
+template <int DIM, int N, int VF, int SF, bool HG, int EPB, int NT>
+__global__ void __launch_bounds__(NT)
+    stage_kernel(const StageArgs<N> p) {
+  using S = StageShape<DIM, N, VF, SF, HG, EPB>;
+  constexpr int NV = S::NV, ND = S::ND, NF = S::NF, NFACE = S::NFACE,
+                NLINE = S::NLINE, NQ = S::NQ;
+  extern __shared__ double smem[];
+  double* us = smem;
+  double* pr = us + S::SM_U;
+  double* fs = pr + S::SM_P;
+  double* dv = fs + S::SM_F;
+  double* alpha_s = dv + S::SM_V;
+
+  const int tid = threadIdx.x;
+  const int64_t e0 = (int64_t)blockIdx.x * EPB;
+  if (e0 >= p.nelem) return;
+  const int ne = (int)min((int64_t)EPB, p.nelem - e0);
+  const double gamma = p.gamma;
+
+  // ---- phase 0: load the contiguous u_in tile ---------------------------
+  {
+    const double2* src = reinterpret_cast<const double2*>(p.u_in + e0 * NV * ND);
+    double2* dst = reinterpret_cast<double2*>(us);
+    const int total = ne * NV * ND;
+    if ((total & 1) == 0) {
+      for (int idx = tid; idx < total / 2; idx += NT) dst[idx] = __ldg(src + idx);
+    } else {
+      for (int idx = tid; idx < total; idx += NT) us[idx] = __ldg(p.u_in + e0 * NV * ND + idx);
+    }
+  }
+  __syncthreads();
+
+  // ---- phase 1: node primitives and HG alpha ----------------------------
+  for (int idx = tid; idx < ne * ND; idx += NT) {
+    const int el = idx / ND, node = idx % ND;
+    double u[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) u[q] = us[(el * NV + q) * ND + node];
+    const NodeState<DIM> s = prepare_node<DIM, VF>(u, gamma);
+    double* P = pr + el * NQ * ND + node;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) P[d * ND] = s.v[d];
+    P[DIM * ND] = s.p;
+    P[(DIM + 1) * ND] = s.beta;
+    P[(DIM + 2) * ND] = s.kin;
+  }
+  if (HG) {
+    for (int el = tid; el < ne; el += NT) {
+      const double a = hg_alpha_2d<N>(us + el * NV * ND, ND, p.basis, p.hg_threshold,
+                                      p.hg_s, p.alpha_min, p.alpha_max);
+      alpha_s[el] = a;
+      if (p.alpha_out) p.alpha_out[e0 + el] = a;
+    }
+  }
+  __syncthreads();
+
+  // ---- phase 2a: face fluxes ----------------------------------------------
+  for (int idx = tid; idx < ne * NFACE * NF; idx += NT) {
+    const int el = idx / (NFACE * NF);
+    const int face = (idx / NF) % NFACE;
+    const int fn = idx % NF;
+    const int dir = face >> 1, side = face & 1;
+    const int64_t e = e0 + el;
+    const ElemIdx<DIM> ei = elem_coords<DIM>(e, p.cells);
+    const int own_node = face_node<DIM, N>(dir, fn, side ? N - 1 : 0);
+    double uo[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) uo[q] = us[(el * NV + q) * ND + own_node];
+    const FaceState<DIM> so = prepare_face<DIM>(uo, gamma);
+    // neighbour along dir
+    ElemIdx<DIM> nb = ei;
+    const int64_t ncell = p.cells[dir];
+    const int64_t pos = ei.i[dir] + (side ? 1 : -1);
+    bool boundary = false;
+    if (pos < 0 || pos >= ncell) {
+      if (p.periodic[dir]) {
+        nb.i[dir] = (pos + ncell) % ncell;
+      } else {
+        boundary = true;
+      }
+    } else {
+      nb.i[dir] = pos;
+    }
+    double f[NV];
+    if (!boundary) {
+      const int64_t en = elem_linear<DIM>(nb, p.cells);
+      const int nb_node = face_node<DIM, N>(dir, fn, side ? 0 : N - 1);
+      double un[NV];
+#pragma unroll
+      for (int q = 0; q < NV; ++q) un[q] = __ldg(p.u_in + (en * NV + q) * ND + nb_node);
+      const FaceState<DIM> sn = prepare_face<DIM>(un, gamma);
+      // normal: Ja^dir of the element on the high side at its low-face node
+      const ElemIdx<DIM>& er = side ? nb : ei;
+      const int r_node = face_node<DIM, N>(dir, fn, 0);
+      double nrm[DIM];
+#pragma unroll
+      for (int c = 0; c < DIM; ++c)
+        nrm[c] = ja_at(p.tab.ja[dir][c], eidx_other<DIM>(er, c, p.cells), ND, r_node);
+      if (side) {
+        surface_flux<DIM, SF>(so, sn, nrm, gamma, f);
+      } else {
+        surface_flux<DIM, SF>(sn, so, nrm, gamma, f);
+      }
+    } else {
+      // boundary_helper.hpp:93-146: own metric at the boundary node;
+      // inner state is the left state on high faces.
+      double nrm[DIM];
+#pragma unroll
+      for (int c = 0; c < DIM; ++c)
+        nrm[c] = ja_at(p.tab.ja[dir][c], eidx_other<DIM>(ei, c, p.cells), ND, own_node);
+      double ub[NV];
+      const int kind = p.bc.kind[face];
+      if (DIM == 2) {
+        const double x = __ldg(p.tab.coord[0] + ei.i[0] * N + (own_node % N));
+        const double y = __ldg(p.tab.coord[1] + ei.i[1] * N + (own_node / N));
+        if (kind == BC_DIRICHLET_DMR) {
+          dmr_state(p.bc, x, y, p.t, ub);
+        } else if (kind == BC_DIRICHLET_CONST) {
+#pragma unroll
+          for (int q = 0; q < NV; ++q) ub[q] = p.bc.state[q];
+        } else if (kind == BC_OUTFLOW) {
+          // outflow_boundary.hpp:79-104: average along the line normal to the face
+#pragma unroll
+          for (int q = 0; q < NV; ++q) {
+            double acc = 0.0;
+#pragma unroll
+            for (int m = 0; m < N; ++m)
+              acc += us[(el * NV + q) * ND + face_node<DIM, N>(dir, fn, m)];
+            ub[q] = acc / (double)N;
+          }
+        } else if (kind == BC_MIXED_DMR_WALL && x < 1.0 / 6.0) {
+          dmr_state(p.bc, x, y, p.t, ub);
+        } else {  // slip wall / wall branch of the mixed BC
+          reflect_state(uo, nrm, ub);
+        }
+      }
+      const FaceState<DIM> sb = prepare_face<DIM>(ub, gamma);
+      if (side) {
+        surface_flux<DIM, SF>(so, sb, nrm, gamma, f);
+      } else {
+        surface_flux<DIM, SF>(sb, so, nrm, gamma, f);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < NV; ++q) fs[((el * NFACE + face) * NV + q) * NF + fn] = f[q];
+  }
+
+  // ---- phase 2b: volume integral, one line per thread --------------------
+  for (int idx = tid; idx < ne * NLINE; idx += NT) {
+    const int el = idx / NLINE;
+    const int dir = (idx % NLINE) / NF;
+    const int line = idx % NF;
+    const int64_t e = e0 + el;
+    const ElemIdx<DIM> ei = elem_coords<DIM>(e, p.cells);
+    const double* U = us + el * NV * ND;
+    const double* P = pr + el * NQ * ND;
+    double ja[N][DIM];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      const double* tab = p.tab.ja[dir][c] + eidx_other<DIM>(ei, c, p.cells) * ND;
+#pragma unroll
+      for (int m = 0; m < N; ++m) ja[m][c] = __ldg(tab + line_node<DIM, N>(dir, line, m));
+    }
+    double acc[N][NV];
+#pragma unroll
+    for (int m = 0; m < N; ++m)
+#pragma unroll
+      for (int q = 0; q < NV; ++q) acc[m][q] = 0.0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      const int ni = line_node<DIM, N>(dir, line, i);
+      NodeState<DIM> Li;
+      Li.rho = U[ni];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) Li.v[d] = P[d * ND + ni];
+      Li.p = P[DIM * ND + ni];
+      Li.beta = P[(DIM + 1) * ND + ni];
+      Li.kin = P[(DIM + 2) * ND + ni];
+#pragma unroll
+      for (int k = i + 1; k < N; ++k) {
+        const int nk = line_node<DIM, N>(dir, line, k);
+        NodeState<DIM> Rk;
+        Rk.rho = U[nk];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) Rk.v[d] = P[d * ND + nk];
+        Rk.p = P[DIM * ND + nk];
+        Rk.beta = P[(DIM + 1) * ND + nk];
+        Rk.kin = P[(DIM + 2) * ND + nk];
+        double nrm[DIM];
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) nrm[c] = 0.5 * (ja[i][c] + ja[k][c]);
+        double f[NV];
+        volume_flux<DIM, VF>(Li, Rk, nrm, p.inv_gm1, f);
+        const double dik = p.basis.Dsplit[i][k];
+        const double dki = p.basis.Dsplit[k][i];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+          acc[i][q] += dik * f[q];
+          acc[k][q] += dki * f[q];
+        }
+      }
+    }
+    if (HG) {
+      const double alpha = alpha_s[el];
+      if (fabs(alpha - 0.0) > p.atol) {
+        // volume_flux.hpp:830-841: (1 - alpha) * DG + alpha * FV
+        const double one_m = 1.0 - alpha;
+#pragma unroll
+        for (int m = 0; m < N; ++m)
+#pragma unroll
+          for (int q = 0; q < NV; ++q) acc[m][q] *= one_m;
+        // volume_flux.hpp:457-509: LLF on subcell normals along the line
+        FaceState<DIM> sl;
+        {
+          double uu[NV];
+          const int n0 = line_node<DIM, N>(dir, line, 0);
+#pragma unroll
+          for (int q = 0; q < NV; ++q) uu[q] = U[q * ND + n0];
+          sl = prepare_face<DIM>(uu, gamma);
+        }
+#pragma unroll
+        for (int fi = 1; fi < N; ++fi) {
+          double uu[NV];
+          const int nr = line_node<DIM, N>(dir, line, fi);
+#pragma unroll
+          for (int q = 0; q < NV; ++q) uu[q] = U[q * ND + nr];
+          const FaceState<DIM> sr = prepare_face<DIM>(uu, gamma);
+          double nrm[DIM];
+#pragma unroll
+          for (int c = 0; c < DIM; ++c)
+            nrm[c] = __ldg(p.tab.fv[dir][c] +
+                           eidx_other<DIM>(ei, c, p.cells) * (N - 1) * N + (fi - 1) * N + line);
+          double f[NV];
+          llf_flux<DIM>(sl, sr, nrm, f);
+          const double wl = alpha * p.basis.inv_w[fi - 1];
+          const double wr = alpha * p.basis.inv_w[fi];
+#pragma unroll
+          for (int q = 0; q < NV; ++q) {
+            acc[fi - 1][q] += wl * f[q];
+            acc[fi][q] -= wr * f[q];
+          }
+          sl = sr;
+        }
+      }
+    }
+    double* V = dv + (el * DIM + dir) * NV * ND;
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+      const int nm = line_node<DIM, N>(dir, line, m);
+#pragma unroll
+      for (int q = 0; q < NV; ++q) V[q * ND + nm] = acc[m][q];
+    }
+  }
+  __syncthreads();
+
+  // ---- phase 3: lift, -1/J, SSPRK3 combination, store ---------------------
+  bool bad = false;
+  for (int idx = tid; idx < ne * NV * ND; idx += NT) {
+    const int el = idx / (NV * ND);
+    const int q = (idx / ND) % NV;
+    const int node = idx % ND;
+    const int64_t e = e0 + el;
+    const ElemIdx<DIM> ei = elem_coords<DIM>(e, p.cells);
+    double du = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) du += dv[((el * DIM + d) * NV + q) * ND + node];
+    const int in = node % N;
+    const int jn = (node / N) % N;
+    const int kn = (DIM == 3) ? node / (N * N) : 0;
+    const int pos[3] = {in, jn, kn};
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      // face node index of this node on the faces normal to d
+      int fn;
+      if (DIM == 2) {
+        fn = (d == 0) ? jn : in;
+      } else {
+        fn = (d == 0) ? (jn + N * kn) : ((d == 1) ? (in + N * kn) : (in + N * jn));
+      }
+      if (pos[d] == 0) du -= fs[((el * NFACE + 2 * d) * NV + q) * NF + fn] * p.basis.lhat_l0;
+      if (pos[d] == N - 1) du += fs[((el * NFACE + 2 * d + 1) * NV + q) * NF + fn] * p.basis.lhat_rN;
+    }
+    double jdet = __ldg(p.tab.jdiag[0] + ei.i[0] * N + in);
+    if (DIM == 2) {
+      jdet = jdet * __ldg(p.tab.jdiag[1] + ei.i[1] * N + jn);
+    } else {
+      jdet = jdet * (__ldg(p.tab.jdiag[1] + ei.i[1] * N + jn) *
+                     __ldg(p.tab.jdiag[2] + ei.i[2] * N + kn));
+    }
+    du = du * (-(1.0 / jdet));
+    double val = p.c * du;
+    if (p.b != 0.0) val = p.b * us[idx] + val;
+    if (p.a != 0.0) val = p.a * __ldg(p.u_n + e0 * NV * ND + idx) + val;
+    bad |= !isfinite(val);
+    p.out[e0 * NV * ND + idx] = val;
+  }
+  if (bad) atomicOr(p.nonfinite, 1u);
+}
+
+}  // namespace dgsem

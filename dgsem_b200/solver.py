@@ -1,0 +1,385 @@
+"""Host-side mirror of the reference's solver interface over the C ABI.
+
+Names and argument meaning follow RetrO598/DGSEM:
+  StructuredMesh(domain_left, domain_right, n_cells)   mesh/structured_mesh.hpp:10-71
+  LobattoLegendreBasis(polydeg)                         polynomial_basis/basis.hpp:12-182
+  CompressibleEuler2D/3D, CompressibleNavierStokes2D    equations/*.hpp
+  ChandrashekarFlux, LaxFriedrichsFlux (+ RanochaFlux, KennedyGruberFlux, HLLCFlux)
+  VolumeIntegralSplitForm, VolumeIntegralShockCapturingHG, HGIndicator
+                                                        space_integral/volume_flux.hpp:686-879
+  PeriodicBC, DirichletBC, OutflowBC, MixedDirichletSlipWallBC, BoundarySet
+                                                        boundary_condition/*.hpp
+  StructuredSolver(eq, basis, volume, surface, mesh, boundaries)
+      .initialize(ic, sol) .calc_rhs(sol, t) .set_indicator_parameters(...)
+      .get_ndofs()                                      solver/structured_solver.hpp:18-143
+  Solution(mesh, basis, eq) .state() .rhs() .clone_shape()
+                                                        containers/solution_container.hpp:157-234
+  SSPRK3(sol, mesh, final_time) .step(solver, sol, dt) .solve(solver, sol, dt)
+                                                        time_integrator/SSPRK3.hpp:145-187
+Templates become descriptor objects; state arrays are caller-visible CUDA
+tensors in the device layout u[e][var][node] (include/dgsem_b200.h).  Every
+compute call runs the CUDA kernels of libdgsem_b200.so; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+
+import torch
+
+from . import _capi as C
+
+
+# ---------------------------------------------------------------- mesh/basis
+@dataclass
+class StructuredMesh:
+    domain_left: tuple
+    domain_right: tuple
+    n_cells: tuple
+
+    @property
+    def ndims(self) -> int:
+        return len(self.n_cells)
+
+    def get_num_cells(self):
+        return tuple(self.n_cells)
+
+    def get_nelem(self) -> int:
+        return int(math.prod(self.n_cells))
+
+
+@dataclass(frozen=True)
+class LobattoLegendreBasis:
+    polydeg: int
+
+    @property
+    def NNodes(self) -> int:
+        return self.polydeg + 1
+
+
+# ---------------------------------------------------------------- equations
+@dataclass(frozen=True)
+class CompressibleEuler2D:
+    gamma: float = 1.4
+    NDIMS = 2
+    NVARS = 4
+    code = C.EULER_2D
+
+
+@dataclass(frozen=True)
+class CompressibleEuler3D:
+    gamma: float = 1.4
+    NDIMS = 3
+    NVARS = 5
+    code = C.EULER_3D
+
+
+@dataclass(frozen=True)
+class CompressibleNavierStokes2D:
+    gamma: float = 1.4
+    mu: float = 5.0e-3
+    prandtl: float = 0.73
+    NDIMS = 2
+    NVARS = 4
+    code = C.NAVIER_STOKES_2D
+
+
+# ---------------------------------------------------------------- fluxes
+class ChandrashekarFlux:
+    code = C.VF_CHANDRASHEKAR
+
+
+class RanochaFlux:
+    code = C.VF_RANOCHA
+
+
+class KennedyGruberFlux:
+    code = C.VF_KENNEDY_GRUBER
+
+
+class LaxFriedrichsFlux:
+    code = C.SF_LAX_FRIEDRICHS
+
+
+class HLLCFlux:
+    code = C.SF_HLLC
+
+
+class HGIndicator:
+    """Hennemann-Gassner indicator (subcell_limiting/indicator.hpp)."""
+
+
+@dataclass(frozen=True)
+class VolumeIntegralSplitForm:
+    numerical_flux: type = ChandrashekarFlux
+    code = C.VI_SPLIT_FORM
+
+
+@dataclass(frozen=True)
+class VolumeIntegralShockCapturingHG:
+    numerical_flux: type = ChandrashekarFlux
+    fv_flux: type = LaxFriedrichsFlux
+    indicator: type = HGIndicator
+    code = C.VI_SHOCK_CAPTURING_HG
+
+    def __post_init__(self):
+        if self.fv_flux is not LaxFriedrichsFlux:
+            raise ValueError("the FV subcell flux is LaxFriedrichsFlux")
+
+
+# ---------------------------------------------------------------- boundaries
+class PeriodicBC:
+    code = C.BC_PERIODIC
+
+
+class OutflowBC:
+    code = C.BC_OUTFLOW
+
+
+@dataclass(frozen=True)
+class DirichletBC:
+    """Dirichlet state: a constant conserved state, or "double_mach" for the
+    double Mach reflection state f(x, t) of the reference example."""
+
+    func: object = "double_mach"
+
+    @property
+    def code(self):
+        return C.BC_DIRICHLET_DMR if self.func == "double_mach" else C.BC_DIRICHLET_CONST
+
+
+@dataclass(frozen=True)
+class MixedDirichletSlipWallBC:
+    """Dirichlet (double Mach state) where x < 1/6, reflecting wall elsewhere."""
+
+    func: object = "double_mach"
+    code = C.BC_MIXED_DMR_WALL
+
+
+class SlipWallBC:
+    code = C.BC_SLIP_WALL
+
+
+class BoundarySet:
+    """One boundary condition per face: left, right, bottom, top(, back, front)."""
+
+    def __init__(self, *bcs):
+        self.faces = list(bcs)
+        self.NFACES = len(bcs)
+
+
+# ---------------------------------------------------------------- initial conditions
+@dataclass(frozen=True)
+class KelvinHelmholtzInitial:
+    code = C.IC_KELVIN_HELMHOLTZ
+    params = None
+
+
+@dataclass(frozen=True)
+class DoubleMachReflectionInitial:
+    gamma: float = 1.4
+    code = C.IC_DOUBLE_MACH
+    params = None
+
+
+@dataclass(frozen=True)
+class InviscidTaylorGreenVortex:
+    code = C.IC_TAYLOR_GREEN_3D
+    params = None
+
+
+@dataclass(frozen=True)
+class TaylorGreenVortex2D:
+    p0: float = 1.0 / (1.4 * 0.01)
+    code = C.IC_TAYLOR_GREEN_2D
+
+    @property
+    def params(self):
+        return (self.p0, 0.0, 0.0)
+
+
+@dataclass(frozen=True)
+class IsentropicVortex:
+    beta: float = 5.0
+    center: tuple = (0.0, 0.0)
+    code = C.IC_ISENTROPIC_VORTEX
+
+    @property
+    def params(self):
+        return (self.beta, self.center[0], self.center[1])
+
+
+# ---------------------------------------------------------------- solution
+class Solution:
+    """State (u) and RHS (du) device arrays, shape (nelem, nvars, n^d)."""
+
+    def __init__(self, mesh: StructuredMesh, basis: LobattoLegendreBasis, equations,
+                 device=None):
+        self.mesh, self.basis, self.equations = mesh, basis, equations
+        self.shape = (mesh.get_nelem(), equations.NVARS, basis.NNodes ** mesh.ndims)
+        dev = device or torch.device("cuda", torch.cuda.current_device())
+        self.u = torch.zeros(self.shape, dtype=torch.float64, device=dev)
+        self.du = torch.zeros_like(self.u)
+
+    def state(self) -> torch.Tensor:
+        return self.u
+
+    def rhs(self) -> torch.Tensor:
+        return self.du
+
+    def clone_shape(self) -> "Solution":
+        return Solution(self.mesh, self.basis, self.equations, device=self.u.device)
+
+
+def _ptr(t: torch.Tensor):
+    if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+        raise ValueError("expected a contiguous float64 CUDA tensor")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+# ---------------------------------------------------------------- solver
+class StructuredSolver:
+    def __init__(self, equations, basis: LobattoLegendreBasis, volume_integral,
+                 surface_flux, mesh: StructuredMesh, boundary_set: BoundarySet,
+                 stream: torch.cuda.Stream | None = None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("StructuredSolver needs a CUDA device (no CPU path)")
+        if boundary_set.NFACES != 2 * mesh.ndims:
+            raise ValueError("one boundary condition per mesh face is required "
+                             "(2 for 1D, 4 for 2D, 6 for 3D)")
+        self.eq, self.basis, self.vi, self.sf = equations, basis, volume_integral, surface_flux
+        self.mesh, self.boundary_set = mesh, boundary_set
+        m = C.MeshDesc()
+        m.ndims = mesh.ndims
+        m.polydeg = basis.polydeg
+        for a in range(3):
+            m.n_cells[a] = int(mesh.n_cells[a]) if a < mesh.ndims else 1
+            m.domain_left[a] = float(mesh.domain_left[a]) if a < mesh.ndims else 0.0
+            m.domain_right[a] = float(mesh.domain_right[a]) if a < mesh.ndims else 1.0
+        s = C.SchemeDesc()
+        s.equation = equations.code
+        s.volume_flux = volume_integral.numerical_flux.code
+        s.surface_flux = surface_flux.code
+        s.volume_integral = volume_integral.code
+        for f, bc in enumerate(boundary_set.faces):
+            s.bc[f] = bc.code
+            if isinstance(bc, DirichletBC) and bc.func != "double_mach":
+                for q, v in enumerate(bc.func):
+                    s.bc_state[q] = float(v)
+        s.gamma = equations.gamma
+        s.mu = getattr(equations, "mu", 0.0)
+        s.prandtl = getattr(equations, "prandtl", 0.72)
+        s.alpha_max, s.alpha_min, s.alpha_smooth = 0.5, 0.001, 0
+        self._mesh_desc, self._scheme_desc = m, s
+        self.stream = stream or torch.cuda.current_stream()
+        h = ctypes.c_void_p()
+        C.check(C.lib().dgsem_ctx_create(ctypes.byref(m), ctypes.byref(s),
+                                         ctypes.c_void_p(self.stream.cuda_stream),
+                                         ctypes.byref(h)), "dgsem_ctx_create")
+        self._ctx = h
+
+    def __del__(self):
+        ctx = getattr(self, "_ctx", None)
+        if ctx is not None and ctx.value:
+            C.lib().dgsem_ctx_destroy(ctx)
+            self._ctx = None
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._ctx
+
+    def get_ndofs(self) -> int:
+        return self.basis.NNodes ** self.mesh.ndims
+
+    def set_indicator_parameters(self, alpha_max: float, alpha_min: float,
+                                 alpha_smooth: bool = False) -> None:
+        C.check(C.lib().dgsem_set_indicator_parameters(self._ctx, alpha_max, alpha_min,
+                                                       int(alpha_smooth)),
+                "dgsem_set_indicator_parameters")
+
+    def initialize(self, initial_condition, sol: Solution) -> None:
+        params = initial_condition.params
+        arr = (ctypes.c_double * 3)(*params) if params is not None else None
+        C.check(C.lib().dgsem_initial_condition(self._ctx, initial_condition.code, arr,
+                                                _ptr(sol.u)), "dgsem_initial_condition")
+
+    def calc_rhs(self, sol: Solution, time: float) -> None:
+        C.check(C.lib().dgsem_rhs(self._ctx, _ptr(sol.u), _ptr(sol.du), float(time)),
+                "dgsem_rhs")
+
+    def rhs(self, u: torch.Tensor, du: torch.Tensor, time: float = 0.0) -> None:
+        C.check(C.lib().dgsem_rhs(self._ctx, _ptr(u), _ptr(du), float(time)), "dgsem_rhs")
+
+    def indicator(self, u: torch.Tensor):
+        """HG alpha per element and troubled-cell flags (uint8)."""
+        n = self.mesh.get_nelem()
+        alpha = torch.empty(n, dtype=torch.float64, device=u.device)
+        flags = torch.empty(n, dtype=torch.uint8, device=u.device)
+        C.check(C.lib().dgsem_indicator(self._ctx, _ptr(u), ctypes.c_void_p(alpha.data_ptr()),
+                                        ctypes.c_void_p(flags.data_ptr())), "dgsem_indicator")
+        return alpha, flags
+
+    def to_reference_layout(self, u: torch.Tensor) -> torch.Tensor:
+        out = torch.empty_like(u)
+        C.check(C.lib().dgsem_to_reference_layout(self._ctx, _ptr(u), _ptr(out)),
+                "dgsem_to_reference_layout")
+        return out.reshape(tuple(self.mesh.n_cells) + (u.shape[2], u.shape[1]))
+
+    def from_reference_layout(self, u_ref: torch.Tensor) -> torch.Tensor:
+        n = self.mesh.get_nelem()
+        src = u_ref.contiguous().reshape(n, -1)
+        out = torch.empty((n, self.eq.NVARS, self.get_ndofs()), dtype=torch.float64,
+                          device=u_ref.device)
+        C.check(C.lib().dgsem_from_reference_layout(self._ctx, _ptr(src), _ptr(out)),
+                "dgsem_from_reference_layout")
+        return out
+
+    def check_finite(self) -> None:
+        C.check(C.lib().dgsem_check_finite(self._ctx), "dgsem_check_finite")
+
+    def launch_count(self) -> int:
+        c = ctypes.c_int64()
+        C.check(C.lib().dgsem_launch_count(self._ctx, ctypes.byref(c)), "dgsem_launch_count")
+        return c.value
+
+
+# ---------------------------------------------------------------- time integration
+class SSPRK3:
+    """Shu-Osher SSPRK3 with each stage one fused kernel (SSPRK3.hpp:145-187)."""
+
+    def __init__(self, sol: Solution, mesh: StructuredMesh, final_time: float = 0.0):
+        self.mesh = mesh
+        self.time = 0.0
+        self.final_time = final_time
+        self.iter = 0
+        self.has_nan = False
+        self.observers = []
+        self.tmp1 = sol.clone_shape()
+        self.tmp2 = sol.clone_shape()
+
+    def add_observer(self, observer) -> None:
+        self.observers.append(observer)
+
+    def step(self, solver: StructuredSolver, sol: Solution, dt: float) -> None:
+        L, h = C.lib(), solver.handle
+        t = self.time
+        C.check(L.dgsem_ssprk3_stage(h, 1, None, _ptr(sol.u), _ptr(self.tmp1.u), t, dt), "stage 1")
+        C.check(L.dgsem_ssprk3_stage(h, 2, _ptr(sol.u), _ptr(self.tmp1.u), _ptr(self.tmp2.u),
+                                     t, dt), "stage 2")
+        C.check(L.dgsem_ssprk3_stage(h, 3, _ptr(sol.u), _ptr(self.tmp2.u), _ptr(sol.u), t, dt),
+                "stage 3")
+
+    def solve(self, solver: StructuredSolver, sol: Solution, dt: float) -> None:
+        """integrator_base.hpp:21-40: fixed dt until final_time, NaN stops."""
+        while self.time < self.final_time:
+            for obs in self.observers:
+                obs(self.iter, self.time, sol)
+            self.step(solver, sol, dt)
+            self.time += dt
+            self.iter += 1
+            try:
+                solver.check_finite()
+            except C.DgsemError:
+                self.has_nan = True
+                break

@@ -1,0 +1,205 @@
+/*
+ * dgsem_b200 -- B200-native (sm_100a) FP64 DGSEM right-hand side and fused
+ * SSPRK3 stage update behind a plain C ABI.
+ *
+ * This ABI replaces the reference's compile-time plugin surface for the hot
+ * path (RetrO598/DGSEM):
+ *   StructuredSolver<Equations, Basis, VolumeFlux, SurfaceFlux, Mesh, BCs>
+ *     ::calc_rhs(Solution&, T time)      src/solver/structured_solver.hpp:466-480
+ *     ::set_indicator_parameters(...)    src/solver/structured_solver.hpp:118-123
+ *     ::get_ndofs()                      src/solver/structured_solver.hpp:125
+ *   SSPRK3<T, Solver, Mesh, Solution>::step(solver, sol, dt)
+ *                                        src/time_integrator/SSPRK3.hpp:159-181
+ *   HGIndicator<Basis, Eq>::operator()   src/subcell_limiting/indicator.hpp:337-418
+ *   InitialFunctor::apply                src/boundary_condition/initial_functor.hpp:33-59
+ * The template parameters become descriptor enums: equation
+ * (compressible_euler2D/3D, compressible_navier_stokes2D), two-point volume
+ * flux (ChandrashekarFlux + Ranocha, Kennedy-Gruber), surface flux
+ * (LaxFriedrichsFlux + 2D HLLC), volume integral (VolumeIntegralSplitForm /
+ * VolumeIntegralShockCapturingHG) and one boundary condition per mesh face
+ * (BoundarySet of PeriodicBC, DirichletBC, OutflowBC,
+ * MixedDirichletSlipWallBC; src/boundary_condition/*.hpp).
+ *
+ * Data layout on the device (all FP64, caller-owned):
+ *   state u[e][var][node], e = ie + nx*(je + ny*ke), node = in + n*(jn + n*kn)
+ * (node numbering = reference local_dof, src/utils/local_dof.hpp:9-19).
+ * dgsem_to_reference_layout / dgsem_from_reference_layout convert to and from
+ * the reference's logical u(i, j[, k], dof, var).
+ *
+ * All pointers passed to compute entry points are DEVICE pointers unless the
+ * name says host.  Every call is asynchronous on the context's stream unless
+ * documented otherwise; no entry point allocates or synchronises during a
+ * step, so steps can be captured into CUDA graphs.  Errors are returned as
+ * dgsem_status, never by aborting.
+ */
+#ifndef DGSEM_B200_H_
+#define DGSEM_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum dgsem_status {
+  DGSEM_OK = 0,
+  DGSEM_ERR_INVALID_ARG = 1,
+  DGSEM_ERR_UNSUPPORTED = 2,
+  DGSEM_ERR_CUDA = 3,
+  DGSEM_ERR_NONFINITE = 4,
+  DGSEM_ERR_TIMEOUT = 5,
+  DGSEM_ERR_ALLOC = 6
+} dgsem_status;
+
+typedef enum dgsem_equation {
+  DGSEM_EULER_2D = 0,          /* equations/compressible_euler2D.hpp */
+  DGSEM_EULER_3D = 1,          /* equations/compressible_euler3D.hpp */
+  DGSEM_NAVIER_STOKES_2D = 2   /* equations/compressible_navier_stokes2D.hpp */
+} dgsem_equation;
+
+typedef enum dgsem_volume_flux {
+  DGSEM_VF_CHANDRASHEKAR = 0,  /* base/numerical_flux.hpp:436-594 */
+  DGSEM_VF_RANOCHA = 1,        /* not in the reference: Ranocha (2018/2020) */
+  DGSEM_VF_KENNEDY_GRUBER = 2  /* not in the reference: Kennedy-Gruber (2008) */
+} dgsem_volume_flux;
+
+typedef enum dgsem_surface_flux {
+  DGSEM_SF_LAX_FRIEDRICHS = 0, /* base/numerical_flux.hpp:39-228 */
+  DGSEM_SF_HLLC = 1            /* 2D normal-rotated form of numerical_flux.hpp:283-378 */
+} dgsem_surface_flux;
+
+typedef enum dgsem_volume_integral {
+  DGSEM_VI_SPLIT_FORM = 0,         /* space_integral/volume_flux.hpp:686-739 */
+  DGSEM_VI_SHOCK_CAPTURING_HG = 1  /* space_integral/volume_flux.hpp:741-879 */
+} dgsem_volume_integral;
+
+typedef enum dgsem_bc_kind {
+  DGSEM_BC_PERIODIC = 0,          /* periodic_boundary.hpp:9-22 */
+  DGSEM_BC_DIRICHLET_DMR = 1,     /* DirichletBC(double-Mach state f(x,t)) */
+  DGSEM_BC_OUTFLOW = 2,           /* outflow_boundary.hpp:57-110 */
+  DGSEM_BC_MIXED_DMR_WALL = 3,    /* MixedDirichletSlipWallBC, Dirichlet for x < 1/6 */
+  DGSEM_BC_DIRICHLET_CONST = 4,   /* DirichletBC with a constant state */
+  DGSEM_BC_SLIP_WALL = 5          /* reflecting wall (MixedDirichletSlipWallBC wall branch) */
+} dgsem_bc_kind;
+
+typedef enum dgsem_initial_kind {
+  DGSEM_IC_KELVIN_HELMHOLTZ = 0,  /* examples/Euler2D/kelvin_helmholtz_hg */
+  DGSEM_IC_DOUBLE_MACH = 1,       /* examples/Euler2D/double_mach_reflection:9-32 */
+  DGSEM_IC_TAYLOR_GREEN_3D = 2,   /* examples/Euler3D/inviscid_tgv:18-35 */
+  DGSEM_IC_TAYLOR_GREEN_2D = 3,   /* params[0] = p0 */
+  DGSEM_IC_ISENTROPIC_VORTEX = 4  /* params = {beta, x0, y0} */
+} dgsem_initial_kind;
+
+typedef struct dgsem_mesh_desc {
+  int ndims;                 /* 2 or 3 */
+  int polydeg;               /* N; nodes per direction n = N + 1 (1 <= N <= 7) */
+  int64_t n_cells[3];        /* elements per direction (unused entries ignored) */
+  double domain_left[3];     /* StructuredMesh domain_left */
+  double domain_right[3];    /* StructuredMesh domain_right */
+} dgsem_mesh_desc;
+
+typedef struct dgsem_scheme_desc {
+  int equation;              /* dgsem_equation */
+  int volume_flux;           /* dgsem_volume_flux (two-point flux of the split form) */
+  int surface_flux;          /* dgsem_surface_flux */
+  int volume_integral;       /* dgsem_volume_integral */
+  int bc[6];                 /* dgsem_bc_kind per face: left, right, bottom, top, back, front */
+  double bc_state[4];        /* conserved state for DGSEM_BC_DIRICHLET_CONST */
+  double gamma;              /* ratio of specific heats */
+  double mu;                 /* dynamic viscosity (Navier-Stokes) */
+  double prandtl;            /* Prandtl number (Navier-Stokes) */
+  double alpha_max;          /* set_indicator_parameters: alpha_max (default 0.5) */
+  double alpha_min;          /* alpha_min (default 0.001) */
+  int alpha_smooth;          /* stored, unused (as in the reference) */
+} dgsem_scheme_desc;
+
+typedef struct dgsem_ctx dgsem_ctx;
+
+/* Human-readable name of a status code (static string). */
+const char* dgsem_status_string(dgsem_status s);
+
+/* Creates a solver context: basis and metric tables, stage temporaries and
+ * the alpha buffer live in the context (replaces the StructuredSolver
+ * constructors, structured_solver.hpp:36-58, and StructuredElementInitializer,
+ * data_container.hpp:729-772).  `stream` is a cudaStream_t (NULL = legacy
+ * default stream).  Synchronous; allocates device memory. */
+dgsem_status dgsem_ctx_create(const dgsem_mesh_desc* mesh,
+                              const dgsem_scheme_desc* scheme, void* stream,
+                              dgsem_ctx** out);
+dgsem_status dgsem_ctx_destroy(dgsem_ctx* ctx);
+dgsem_status dgsem_ctx_set_stream(dgsem_ctx* ctx, void* stream);
+
+/* Sizes: number of elements, nodes per element (n^d), variables, and the
+ * total number of doubles of one state array (elements * nodes * nvars).
+ * get_ndofs() of the reference is nodes_per_element. */
+dgsem_status dgsem_get_sizes(const dgsem_ctx* ctx, int64_t* n_elements,
+                             int* nodes_per_element, int* nvars,
+                             int64_t* state_len);
+
+/* set_indicator_parameters(alpha_max, alpha_min, alpha_smooth). */
+dgsem_status dgsem_set_indicator_parameters(dgsem_ctx* ctx, double alpha_max,
+                                            double alpha_min, int alpha_smooth);
+
+/* du = RHS(u, t): calc_rhs (structured_solver.hpp:466-480). */
+dgsem_status dgsem_rhs(dgsem_ctx* ctx, const double* u, double* du, double t);
+
+/* One fused SSPRK3 stage: u_out = a*u_n + b*u_in + c*dt*RHS(u_in, t_stage),
+ * stage 1: (0, 1, 1) at t, stage 2: (3/4, 1/4, 1/4) at t+dt,
+ * stage 3: (1/3, 2/3, 2/3) at t+dt/2 (SSPRK3.hpp:159-181).  u_out may alias
+ * u_n (stage 3 writes in place like the reference) but not u_in. */
+dgsem_status dgsem_ssprk3_stage(dgsem_ctx* ctx, int stage, const double* u_n,
+                                const double* u_in, double* u_out, double t,
+                                double dt);
+
+/* One SSPRK3 step in place (three fused stage launches; temporaries owned by
+ * the context). */
+dgsem_status dgsem_ssprk3_step(dgsem_ctx* ctx, double* u, double t, double dt);
+
+/* nsteps SSPRK3 steps in place, t_k = t0 + k*dt. */
+dgsem_status dgsem_ssprk3_steps(dgsem_ctx* ctx, double* u, double t0,
+                                double dt, int nsteps);
+
+/* Hennemann-Gassner blending factor per element and troubled-cell flag
+ * (alpha > max(100 eps, eps^0.75), volume_flux.hpp:772-773).  Either output
+ * may be NULL. */
+dgsem_status dgsem_indicator(dgsem_ctx* ctx, const double* u, double* alpha,
+                             uint8_t* flags);
+
+/* Nodal initial condition (InitialFunctor at the reference node
+ * coordinates).  params may be NULL when the kind takes none. */
+dgsem_status dgsem_initial_condition(dgsem_ctx* ctx, int kind,
+                                     const double* params, double* u);
+
+/* Layout conversions between the device layout and the reference's logical
+ * LayoutRight u(i, j[, k], dof, var). */
+dgsem_status dgsem_to_reference_layout(dgsem_ctx* ctx, const double* u,
+                                       double* u_ref);
+dgsem_status dgsem_from_reference_layout(dgsem_ctx* ctx, const double* u_ref,
+                                         double* u);
+
+/* Non-finite detection: every stage kernel ORs a device flag when it writes a
+ * NaN/Inf.  This call synchronises the stream, returns DGSEM_ERR_NONFINITE if
+ * the flag is set, and clears it. */
+dgsem_status dgsem_check_finite(dgsem_ctx* ctx);
+
+/* Number of kernel launches issued by this context so far (diagnostics). */
+dgsem_status dgsem_launch_count(const dgsem_ctx* ctx, int64_t* count);
+
+/* Host-side copies of the basis tables (nodes, weights, inv_weights,
+ * lhat(-1), lhat(+1), D, Dsplit, Dhat, inverse Legendre Vandermonde; the
+ * n x n tables row-major) for polydeg N; out needs 5n + 4n^2 doubles.
+ * No GPU needed. */
+dgsem_status dgsem_basis_tables_host(int polydeg, double* out);
+
+/* Host-side reconstruction of the per-node metrics the kernels use
+ * (contravariant vectors Ja^a_c and 1/J) in the reference's logical layout
+ * ja(cells..., dof, a, c), inv_j(cells..., dof).  No GPU needed. */
+dgsem_status dgsem_metrics_host(const dgsem_mesh_desc* mesh, double* ja,
+                                double* inv_j);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DGSEM_B200_H_ */

@@ -790,7 +790,11 @@ def hg_alpha(s: Scheme, u):
     energy = np.maximum(e1, e2)
     threshold = 0.5 * 10.0 ** (-1.8 * float(n) ** 0.25)
     sfac = math.log((1.0 - 0.0001) / 0.0001)
-    alpha = 1.0 / (1.0 + np.exp(-sfac / threshold * (energy - threshold)))
+    # libm exp per element (numpy's vectorised exp may differ by an ulp from
+    # the C library the reference calls, indicator.hpp:409)
+    arg = -sfac / threshold * (energy - threshold)
+    ex = np.vectorize(math.exp, otypes=[np.float64])(arg)
+    alpha = 1.0 / (1.0 + ex)
     alpha = np.where(alpha < s.alpha_min, 0.0, alpha)
     alpha = np.where(alpha > 1.0 - s.alpha_min, 1.0, alpha)
     return np.minimum(s.alpha_max, alpha)
