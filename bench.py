@@ -1,0 +1,420 @@
+#!/usr/bin/env python
+"""DGSEM RHS benchmark: FP64 DOF-updates/s per RHS on one B200 (or N replicas).
+
+Workload (default): 3D Euler Taylor-Green vortex,
+periodic 16^3 elements on [0, 2pi]^3, N = 3 (4^3 LGL nodes), Mach 0.1,
+Kennedy-Gruber split-form volume flux, LLF surface flux, SSPRK3 with the
+reference TGV time step rule.  A "step" is one SSPRK3 step = 3 fused stage
+kernels = 3 RHS evaluations; DOF-updates/s = elements * n^3 * 3 / step time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl dgsem_b200|reference]
+                  [--workload tgv16|tgv32|tgv64|kh64|kh1024|dmr]
+
+The device arm times every step with CUDA events on the solver's stream and
+flushes L2 (a 256 MiB write) before every step outside the timed events.
+`e2e` repeats the step through the host-buffer C-ABI entry point
+(dgsem_ssprk3_steps_host: pinned host state -> device, step, -> host).
+`roofline` uses the fused stage kernel's per-launch event times and its
+algorithmic bytes (state reads + writes, 8*NVARS*8/3 B per DOF per stage).
+`--impl reference` times the reference solver's own CPU code (compiled with
+the project's Kokkos shim and OpenMP, oracle/_ref) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (ndims, polydeg, cells, left, right, volume flux, surface flux, ic, vi, bcs)
+    "tgv16": (3, 3, (16, 16, 16), (0.0,) * 3, (2 * math.pi,) * 3, "kennedy_gruber", "llf",
+              "tgv3d", "split", "periodic"),
+    "tgv32": (3, 3, (32, 32, 32), (0.0,) * 3, (2 * math.pi,) * 3, "kennedy_gruber", "llf",
+              "tgv3d", "split", "periodic"),
+    "tgv64": (3, 3, (64, 64, 64), (0.0,) * 3, (2 * math.pi,) * 3, "kennedy_gruber", "llf",
+              "tgv3d", "split", "periodic"),
+    "kh64": (2, 3, (64, 64), (-1.0, -1.0), (1.0, 1.0), "ranocha", "llf", "kh", "split",
+             "periodic"),
+    "kh1024": (2, 3, (1024, 1024), (-1.0, -1.0), (1.0, 1.0), "ranocha", "llf", "kh", "split",
+               "periodic"),
+    "dmr": (2, 3, (240, 60), (0.0, 0.0), (4.0, 1.0), "chandrashekar", "hllc", "dmr", "hg",
+            "dmr"),
+}
+VF_CODE = {"chandrashekar": 0, "ranocha": 1, "kennedy_gruber": 2}
+SF_CODE = {"llf": 0, "hllc": 1}
+
+
+def time_step_size(name: str) -> float:
+    nd, N, cells, left, right = WORKLOADS[name][:5]
+    if name.startswith("tgv"):
+        # examples/Euler3D/inviscid_tgv/inviscid_tgv.cpp:111-117 with order 3
+        dx = min((right[a] - left[a]) / cells[a] for a in range(3))
+        return 0.1 * dx / 2.0 / (3.0 * (2 * 3 + 1))
+    if name == "dmr":
+        # CFL 0.4, lambda_max = 12 (double_mach_reflection_structured.cpp:141-148)
+        return 0.4 * min(4.0 / cells[0], 1.0 / cells[1]) / ((2.0 * (N + 1) - 1.0) * 12.0)
+    # KH: CFL 0.5 with lambda_max from the initial state (|v| + c <= 1.84)
+    dx = min((right[a] - left[a]) / cells[a] for a in range(nd))
+    return 0.5 * dx / ((2.0 * (N + 1) - 1.0) * 1.84)
+
+
+def bytes_per_dof_stage(nvars: int) -> float:
+    # stage 1 reads 1 state and writes 1; stages 2, 3 read 2 and write 1
+    return 8.0 * nvars * 8.0 / 3.0
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic(workload: str):
+    """Per-launch DRAM bytes of the stage kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", f"stage_kernel_{workload}.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.proc = None
+        self.dev = device_index
+        self.out = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# reference arm / CPU baseline
+# ---------------------------------------------------------------------------
+def reference_rate(workload: str, budget_s: float, max_steps: int):
+    """Times the reference solver's CPU code (oracle/_ref) on the workload."""
+    from oracle import dgsem_oracle as do
+    from oracle import ref_binding as rb
+    nd, N, cells, left, right, vf, sf, ic, vi, bcs = WORKLOADS[workload]
+    if nd == 3:
+        kind = rb.EULER3D_PERIODIC_SPLIT
+    elif bcs == "dmr":
+        kind = rb.EULER2D_DMR_HG
+    else:
+        kind = rb.EULER2D_PERIODIC_SPLIT
+    rc = rb.RefCase(kind, N, cells, left, right, volume_flux=VF_CODE[vf],
+                    surface_flux=SF_CODE[sf])
+    s_small = None
+    # initial state from the oracle's node coordinates formula at full size
+    s_small = do.Scheme(ndims=nd, polydeg=N, cells=cells, left=left, right=right,
+                        periodic=(bcs == "periodic"), bc=bcs if bcs == "dmr" else "periodic")
+    u = do.initial_state(s_small, ic)
+    dt = time_step_size(workload)
+    u = rc.ssprk3(u, 0.0, dt, 1)  # warm-up step
+    t0 = time.perf_counter()
+    u = rc.ssprk3(u, dt, dt, 1)
+    one = time.perf_counter() - t0
+    n = max(1, min(max_steps, int(budget_s / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    rc.ssprk3(u, 2 * dt, dt, n)
+    el = time.perf_counter() - t0
+    dofs = math.prod(cells) * (N + 1) ** nd
+    threads = rb.lib().dgsem_ref_omp_threads()
+    return dofs * 3 * n / el, n, el, threads
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    nd, N, cells = WORKLOADS[args.workload][:3]
+    try:
+        rate, n, el, threads = reference_rate(args.workload, budget_s=60.0,
+                                              max_steps=max(args.steps, 1))
+    except Exception as exc:  # reference library missing on this machine
+        print(json.dumps({"impl": "reference", "unavailable": f"{type(exc).__name__}: {exc}"}))
+        return 0
+    sample = (f"{n} SSPRK3 steps of the full {args.workload} mesh ({el:.1f} s, time-capped at "
+              f"60 s of the {args.steps} requested); reference src/ compiled with the project's "
+              f"Kokkos shim, OpenMP")
+    line = {
+        "metric": "FP64 DOF-updates/s per RHS", "value": rate, "unit": "DOF-updates/s",
+        "impl": "reference", "n_gpus": args.gpus, "steps": n, "warmup": 1,
+        "ms_per_step": 1e3 * el / n, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(args.workload),
+        "cpu_baseline": {"value": rate, "unit": "DOF-updates/s", "cores": threads,
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": rate, "unit": "DOF-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def workload_config(name: str) -> dict:
+    nd, N, cells, left, right, vf, sf, ic, vi, bcs = WORKLOADS[name]
+    return {"workload": name, "equation": "euler3d" if nd == 3 else "euler2d",
+            "mesh": list(cells), "polydeg": N, "dofs": math.prod(cells) * (N + 1) ** nd,
+            "volume_flux": vf, "surface_flux": sf,
+            "volume_integral": "shock_capturing_hg" if vi == "hg" else "split_form",
+            "boundaries": bcs, "initial_condition": ic, "dt": time_step_size(name),
+            "l2": "flushed (256 MiB write) before every timed step, outside the step events"}
+
+
+# ---------------------------------------------------------------------------
+# device arm
+# ---------------------------------------------------------------------------
+def build_solver(name: str, dev):
+    import dgsem_b200 as D
+    nd, N, cells, left, right, vf, sf, ic, vi, bcs = WORKLOADS[name]
+    mesh = D.StructuredMesh(left, right, cells)
+    eq = D.CompressibleEuler3D(1.4) if nd == 3 else D.CompressibleEuler2D(1.4)
+    flux = {"chandrashekar": D.ChandrashekarFlux, "ranocha": D.RanochaFlux,
+            "kennedy_gruber": D.KennedyGruberFlux}[vf]
+    vint = D.VolumeIntegralShockCapturingHG(flux) if vi == "hg" else D.VolumeIntegralSplitForm(flux)
+    sflux = D.HLLCFlux() if sf == "hllc" else D.LaxFriedrichsFlux()
+    if bcs == "dmr":
+        bset = D.BoundarySet(D.DirichletBC("double_mach"), D.OutflowBC(),
+                             D.MixedDirichletSlipWallBC("double_mach"),
+                             D.DirichletBC("double_mach"))
+    else:
+        bset = D.BoundarySet(*[D.PeriodicBC() for _ in range(2 * nd)])
+    solver = D.StructuredSolver(eq, D.LobattoLegendreBasis(N), vint, sflux, mesh, bset)
+    if vi == "hg":
+        solver.set_indicator_parameters(0.5, 0.001, False)
+    sol = D.Solution(mesh, D.LobattoLegendreBasis(N), eq, device=dev)
+    init = {"tgv3d": D.InviscidTaylorGreenVortex(), "kh": D.KelvinHelmholtzInitial(),
+            "dmr": D.DoubleMachReflectionInitial(1.4)}[ic]
+    solver.initialize(init, sol)
+    return solver, sol
+
+
+def run_device_arm(args):
+    import ctypes
+
+    import torch
+    import torch.distributed as dist
+
+    import dgsem_b200 as D
+    from dgsem_b200 import _capi as C
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    name = args.workload
+    nd, N, cells = WORKLOADS[name][:3]
+    nvars = nd + 2
+    dofs = math.prod(cells) * (N + 1) ** nd
+    dt = time_step_size(name)
+    solver, sol = build_solver(name, dev)
+    integ = D.SSPRK3(sol, solver.mesh, 0.0)
+    stream = solver.stream
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    L = C.lib()
+    h = solver.handle
+    up, t1p, t2p = (ctypes.c_void_p(x.data_ptr()) for x in (sol.u, integ.tmp1.u, integ.tmp2.u))
+
+    def step(t, evs=None):
+        if evs:
+            evs[0].record(stream)
+        C.check(L.dgsem_ssprk3_stage(h, 1, None, up, t1p, t, dt), "stage 1")
+        if evs:
+            evs[1].record(stream)
+        C.check(L.dgsem_ssprk3_stage(h, 2, up, t1p, t2p, t, dt), "stage 2")
+        if evs:
+            evs[2].record(stream)
+        C.check(L.dgsem_ssprk3_stage(h, 3, up, t2p, up, t, dt), "stage 3")
+        if evs:
+            evs[3].record(stream)
+
+    t = 0.0
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step(t)
+            t += dt
+        torch.cuda.synchronize()
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)]
+               for _ in range(args.steps)]
+        sampler = ClockSampler(dev.index)
+        sampler.start()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        launches0 = solver.launch_count()
+        wall0 = time.perf_counter()
+        for k in range(args.steps):
+            flush.fill_(k & 0xFF)
+            step(t, evs[k])
+            t += dt
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - wall0
+        if world > 1:
+            dist.barrier()
+        launches = solver.launch_count() - launches0
+        clocks = sampler.stop()
+        solver.check_finite()
+    step_ms = [e[0].elapsed_time(e[3]) for e in evs]
+    stage_ms = [[e[s].elapsed_time(e[s + 1]) for e in evs] for s in range(3)]
+    total_ms = sum(step_ms)
+    if world > 1:
+        tt = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    value = world * dofs * 3 * args.steps / (total_ms * 1e-3)
+    # roofline of the fused stage kernel
+    bpd = bytes_per_dof_stage(nvars)
+    mean_stage_s = sum(sum(x) for x in stage_ms) / (3 * args.steps) * 1e-3
+    achieved = dofs * bpd / mean_stage_s / 1e9
+    peak, peak_kind = measured_peak()
+    traffic = profile_traffic(name)
+
+    # e2e through the host-buffer C-ABI entry point (pinned host state)
+    n_e2e = max(3, min(args.steps, 200))
+    host = sol.u.detach().to("cpu").pin_memory()
+    hp = ctypes.c_void_p(host.data_ptr())
+    C.check(L.dgsem_ssprk3_steps_host(h, hp, t, dt, 1), "e2e warm-up")
+    e2e_ms = []
+    for k in range(n_e2e):
+        t0 = time.perf_counter()
+        C.check(L.dgsem_ssprk3_steps_host(h, hp, t, dt, 1), "e2e step")
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        t += dt
+    e2e_value = world * dofs * 3 / (statistics.mean(e2e_ms) * 1e-3)
+    state_bytes = dofs * nvars * 8
+
+    # graph-replayed steps (one graph launch = one step), same flush discipline
+    g = ctypes.c_void_p()
+    C.check(L.dgsem_graph_create(h, up, dt, 1, ctypes.byref(g)), "graph create")
+    gev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(min(args.steps, 2000))]
+    with torch.cuda.stream(stream):
+        for k, (a, b) in enumerate(gev):
+            flush.fill_(k & 0xFF)
+            a.record(stream)
+            C.check(L.dgsem_graph_launch(g, t), "graph launch")
+            b.record(stream)
+            t += dt
+        torch.cuda.synchronize()
+    graph_ms = statistics.mean(a.elapsed_time(b) for a, b in gev)
+    L.dgsem_graph_destroy(g)
+
+    line = {
+        "metric": "FP64 DOF-updates/s per RHS", "value": value, "unit": "DOF-updates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (analytic initial condition of the workload)",
+        "config": dict(workload_config(name),
+                       parallelism=("replicas" if world > 1 else "single")),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs"
+                     if peak_kind == "measured" else "fallback 6650 GB/s",
+                     "kernel": "stage_kernel (fused RHS + SSPRK3 stage)",
+                     "algorithmic_bytes_per_launch": dofs * bpd},
+        "e2e": {"value": e2e_value, "unit": "DOF-updates/s", "h2d_bytes_per_step": state_bytes,
+                "d2h_bytes_per_step": state_bytes, "steps": n_e2e,
+                "ms_per_step": statistics.mean(e2e_ms)},
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "details": {"stage_ms_mean": [statistics.mean(x) for x in stage_ms],
+                    "step_ms_median": statistics.median(step_ms),
+                    "graph_step_ms_mean": graph_ms, "wall_s_timed_loop": wall},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            rate, n, el, threads = reference_rate(name, budget_s=args.cpu_budget,
+                                                  max_steps=10 ** 6)
+            line["cpu_baseline"] = {
+                "value": rate, "unit": "DOF-updates/s", "cores": threads, "kind": "reference",
+                "sample": f"{n} SSPRK3 steps of the full {name} mesh in {el:.1f} s; reference "
+                          f"src/ with the project's Kokkos shim, OpenMP"}
+        except Exception as exc:
+            line["cpu_baseline"] = {"value": None, "unavailable": f"{type(exc).__name__}: {exc}"}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="dgsem_b200", choices=["dgsem_b200", "reference"])
+    ap.add_argument("--workload", default="tgv16", choices=list(WORKLOADS))
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_device_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -33,7 +33,8 @@ EXPORTED = [
     "dgsem_rhs", "dgsem_ssprk3_stage", "dgsem_ssprk3_step", "dgsem_ssprk3_steps",
     "dgsem_indicator", "dgsem_initial_condition", "dgsem_to_reference_layout",
     "dgsem_from_reference_layout", "dgsem_check_finite", "dgsem_launch_count",
-    "dgsem_basis_tables_host", "dgsem_metrics_host",
+    "dgsem_basis_tables_host", "dgsem_metrics_host", "dgsem_ssprk3_steps_host",
+    "dgsem_graph_create", "dgsem_graph_launch", "dgsem_graph_destroy",
 ]
 
 
@@ -93,6 +94,10 @@ def lib() -> ctypes.CDLL:
     L.dgsem_basis_tables_host.argtypes = [c.c_int, c.POINTER(c.c_double)]
     L.dgsem_metrics_host.argtypes = [c.POINTER(MeshDesc), c.POINTER(c.c_double),
                                      c.POINTER(c.c_double)]
+    L.dgsem_ssprk3_steps_host.argtypes = [vp, vp, c.c_double, c.c_double, c.c_int]
+    L.dgsem_graph_create.argtypes = [vp, dp, c.c_double, c.c_int, c.POINTER(vp)]
+    L.dgsem_graph_launch.argtypes = [vp, c.c_double]
+    L.dgsem_graph_destroy.argtypes = [vp]
     for name in EXPORTED:
         f = getattr(L, name)
         if name != "dgsem_status_string":

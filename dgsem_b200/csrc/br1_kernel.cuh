@@ -1,0 +1,136 @@
+// BR1 lifted gradient of the Navier-Stokes gradient variables q = (rho, v1,
+// v2, T = p/rho) for 2D periodic meshes: one kernel, one thread per node.
+//   q at nodes                          compressible_navier_stokes2D.hpp:56-69
+//   weak-form volume term with Dhat     parabolic_gradient.hpp:509-532
+//   transform with Ja                   parabolic_gradient.hpp:573-585
+//   interface average q^ = (q- + q+)/2  parabolic_gradient.hpp:620-686
+//   lifting with the element's own face normals, then * 1/J
+//                                       parabolic_gradient.hpp:712-818
+// Output: grad[e][var][dim][node] (4 x 2 x n^2 doubles per element), read by
+// the fused stage kernel for the viscous flux.
+#pragma once
+
+#include "stage_kernel.cuh"
+
+namespace dgsem {
+
+__device__ __forceinline__ void ns_gradient_variables(const double* u, double gamma,
+                                                      double* q) {
+  const double rho = u[0];
+  const double inv_rho = 1.0 / rho;
+  const double v1 = u[1] * inv_rho;
+  const double v2 = u[2] * inv_rho;
+  const double p = (gamma - 1.0) * (u[3] - 0.5 * (u[1] * u[1] + u[2] * u[2]) * inv_rho);
+  q[0] = rho;
+  q[1] = v1;
+  q[2] = v2;
+  q[3] = p * inv_rho;
+}
+
+// Viscous flux -F_v in direction dim (compressible_navier_stokes2D.hpp:71-106;
+// the solver stores -F_v, parabolic_viscous.hpp:383-387).
+__device__ __forceinline__ void ns_neg_viscous_flux(const double* q, const double* gx,
+                                                    const double* gy, double mu,
+                                                    double kappa, int dim, double* f) {
+  const double tau11 = (4.0 * gx[1] - 2.0 * gy[2]) / 3.0;
+  const double tau22 = (4.0 * gy[2] - 2.0 * gx[1]) / 3.0;
+  const double tau12 = gy[1] + gx[2];
+  f[0] = -0.0;
+  if (dim == 0) {
+    f[1] = -(mu * tau11);
+    f[2] = -(mu * tau12);
+    f[3] = -(mu * (q[1] * tau11 + q[2] * tau12 + kappa * gx[3]));
+  } else {
+    f[1] = -(mu * tau12);
+    f[2] = -(mu * tau22);
+    f[3] = -(mu * (q[1] * tau12 + q[2] * tau22 + kappa * gy[3]));
+  }
+}
+
+template <int N>
+struct GradArgs {
+  const double* u;
+  double* grad;
+  int64_t cells[3];
+  int64_t nelem;
+  double gamma;
+  DeviceTables tab;
+  BasisConst<N> basis;
+};
+
+template <int N, int EPB>
+__global__ void __launch_bounds__(EPB* N* N) br1_gradient_kernel(const GradArgs<N> p) {
+  constexpr int ND = N * N, NV = 4, NG = 4;
+  __shared__ double qs[EPB][NG][ND];
+  const int tid = threadIdx.x;
+  const int el = tid / ND;
+  const int node = tid % ND;
+  const int64_t e = (int64_t)blockIdx.x * EPB + el;
+  const bool active = e < p.nelem;
+  double q[NG] = {0, 0, 0, 0};
+  if (active) {
+    double u[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) u[v] = __ldg(p.u + (e * NV + v) * ND + node);
+    ns_gradient_variables(u, p.gamma, q);
+#pragma unroll
+    for (int v = 0; v < NG; ++v) qs[el][v][node] = q[v];
+  }
+  __syncthreads();
+  if (!active) return;
+  const int i = node % N, j = node / N;
+  const ElemIdx<2> ei = elem_coords<2>(e, p.cells);
+  double ja[2][2];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+      ja[a][c] = __ldg(p.tab.ja[a][c] + eidx_other<2>(ei, c, p.cells) * ND + node);
+  double g[NG][2];
+#pragma unroll
+  for (int v = 0; v < NG; ++v) {
+    double gxi = 0.0, geta = 0.0;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      gxi += p.basis.Dhat[i][k] * qs[el][v][j * N + k];
+      geta += p.basis.Dhat[j][k] * qs[el][v][k * N + i];
+    }
+    g[v][0] = ja[0][0] * gxi + ja[1][0] * geta;
+    g[v][1] = ja[0][1] * gxi + ja[1][1] * geta;
+  }
+  // lifting: x faces first, then y faces (parabolic_gradient.hpp:722-744)
+#pragma unroll
+  for (int dir = 0; dir < 2; ++dir) {
+    const int pos = dir == 0 ? i : j;
+    if (pos != 0 && pos != N - 1) continue;
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      if ((side == 0 && pos != 0) || (side == 1 && pos != N - 1)) continue;
+      ElemIdx<2> nb = ei;
+      const int64_t nc = p.cells[dir];
+      nb.i[dir] = (ei.i[dir] + (side ? 1 : nc - 1)) % nc;
+      const int64_t en = elem_linear<2>(nb, p.cells);
+      const int nb_node = dir == 0 ? ((side ? 0 : N - 1) + N * j) : (i + N * (side ? 0 : N - 1));
+      double un[NV], qn[NG];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) un[v] = __ldg(p.u + (en * NV + v) * ND + nb_node);
+      ns_gradient_variables(un, p.gamma, qn);
+      const double factor = side ? p.basis.lhat_rN : -p.basis.lhat_l0;
+#pragma unroll
+      for (int v = 0; v < NG; ++v) {
+        // q^ = 0.5 (q_left + q_right): the left state is the low-side element's
+        const double qhat = side ? 0.5 * (q[v] + qn[v]) : 0.5 * (qn[v] + q[v]);
+#pragma unroll
+        for (int d = 0; d < 2; ++d) g[v][d] += factor * qhat * ja[dir][d];
+      }
+    }
+  }
+  const double inv_j =
+      1.0 / (__ldg(p.tab.jdiag[0] + ei.i[0] * N + i) * __ldg(p.tab.jdiag[1] + ei.i[1] * N + j));
+#pragma unroll
+  for (int v = 0; v < NG; ++v)
+#pragma unroll
+    for (int d = 0; d < 2; ++d) p.grad[((e * NG + v) * 2 + d) * ND + node] = g[v][d] * inv_j;
+}
+
+}  // namespace dgsem

@@ -29,6 +29,8 @@ struct dgsem_ctx {
   std::vector<void*> allocations;
   double* tmp1 = nullptr;  // SSPRK3 stage states
   double* tmp2 = nullptr;
+  double* staging = nullptr;  // device copy for the host-buffer entry point
+  double* tdev = nullptr;     // device clock for graph replay
   double* table_block = nullptr;
   unsigned int* flag = nullptr;
   int64_t launches = 0;
@@ -199,7 +201,12 @@ dgsem_status validate(const dgsem_mesh_desc* m, const dgsem_scheme_desc* s) {
     if (m->ndims != 2) return DGSEM_ERR_UNSUPPORTED;
     if (!(s->alpha_min >= 0.0 && s->alpha_max >= 0.0)) return DGSEM_ERR_INVALID_ARG;
   }
-  if (s->equation == DGSEM_NAVIER_STOKES_2D) return DGSEM_ERR_UNSUPPORTED;
+  if (s->equation == DGSEM_NAVIER_STOKES_2D) {
+    if (s->volume_integral != DGSEM_VI_SPLIT_FORM) return DGSEM_ERR_UNSUPPORTED;
+    for (int f = 0; f < 4; ++f)
+      if (s->bc[f] != DGSEM_BC_PERIODIC) return DGSEM_ERR_UNSUPPORTED;
+    if (!(s->mu >= 0.0) || !(s->prandtl > 0.0)) return DGSEM_ERR_INVALID_ARG;
+  }
   return DGSEM_OK;
 }
 
@@ -246,7 +253,8 @@ dgsem_status dgsem_ctx_create(const dgsem_mesh_desc* mesh,
   const bool hg = scheme->volume_integral == DGSEM_VI_SHOCK_CAPTURING_HG;
   std::unique_ptr<EngineBase> engine;
   try {
-    engine = make_engine(nd, n, scheme->volume_flux, scheme->surface_flux, hg);
+    engine = make_engine(nd, n, scheme->volume_flux, scheme->surface_flux, hg,
+                         scheme->equation == DGSEM_NAVIER_STOKES_2D);
   } catch (...) {
     return DGSEM_ERR_ALLOC;
   }
@@ -338,7 +346,14 @@ dgsem_status dgsem_ctx_create(const dgsem_mesh_desc* mesh,
                    cudaMemcpyHostToDevice);
   ctx->tmp1 = device_alloc<double>(ctx, ctx->state_len, &err);
   ctx->tmp2 = ctx->tmp1 ? device_alloc<double>(ctx, ctx->state_len, &err) : nullptr;
-  ctx->flag = ctx->tmp2 ? device_alloc<unsigned int>(ctx, 1, &err) : nullptr;
+  ctx->staging = ctx->tmp2 ? device_alloc<double>(ctx, ctx->state_len, &err) : nullptr;
+  ctx->tdev = ctx->staging ? device_alloc<double>(ctx, 1, &err) : nullptr;
+  ctx->flag = ctx->tdev ? device_alloc<unsigned int>(ctx, 1, &err) : nullptr;
+  c.grad = nullptr;
+  if (ctx->flag && scheme->equation == DGSEM_NAVIER_STOKES_2D) {
+    c.grad = device_alloc<double>(ctx, (size_t)c.nelem * 8 * ctx->nodes, &err);
+    if (!c.grad) ctx->flag = nullptr;
+  }
   if (!ctx->flag) {
     free_all(ctx);
     delete ctx;
@@ -392,17 +407,19 @@ dgsem_status dgsem_set_indicator_parameters(dgsem_ctx* ctx, double alpha_max,
 
 dgsem_status dgsem_rhs(dgsem_ctx* ctx, const double* u, double* du, double t) {
   if (!ctx || !u || !du || u == du) return DGSEM_ERR_INVALID_ARG;
-  ctx->launches++;
+  ctx->launches += ctx->engine->kernels_per_stage();
   return cuda_status(ctx->engine->stage(ctx->cfg, nullptr, u, du, 0.0, 0.0, 1.0,
-                                        t, nullptr, ctx->stream));
+                                        t, nullptr, nullptr, ctx->stream));
 }
 
-dgsem_status dgsem_ssprk3_stage(dgsem_ctx* ctx, int stage, const double* u_n,
-                                const double* u_in, double* u_out, double t,
-                                double dt) {
+// One SSPRK3 stage (SSPRK3.hpp:162-180).  With t_dev the stage time is
+// *t_dev + t + stage offset (graph replay); otherwise t + stage offset.
+static dgsem_status launch_stage(dgsem_ctx* ctx, int stage, const double* u_n,
+                                 const double* u_in, double* u_out, double t,
+                                 double dt, const double* t_dev,
+                                 cudaStream_t stream) {
   if (!ctx || !u_in || !u_out || u_out == u_in) return DGSEM_ERR_INVALID_ARG;
   double a, b, c, ts;
-  // SSPRK3.hpp:162-180
   if (stage == 1) {
     a = 0.0; b = 1.0; c = dt; ts = t;
   } else if (stage == 2) {
@@ -413,9 +430,16 @@ dgsem_status dgsem_ssprk3_stage(dgsem_ctx* ctx, int stage, const double* u_n,
     return DGSEM_ERR_INVALID_ARG;
   }
   if (stage > 1 && !u_n) return DGSEM_ERR_INVALID_ARG;
-  ctx->launches++;
+  ctx->launches += ctx->engine->kernels_per_stage();
   return cuda_status(ctx->engine->stage(ctx->cfg, u_n, u_in, u_out, a, b, c, ts,
-                                        nullptr, ctx->stream));
+                                        t_dev, nullptr, stream));
+}
+
+dgsem_status dgsem_ssprk3_stage(dgsem_ctx* ctx, int stage, const double* u_n,
+                                const double* u_in, double* u_out, double t,
+                                double dt) {
+  if (!ctx) return DGSEM_ERR_INVALID_ARG;
+  return launch_stage(ctx, stage, u_n, u_in, u_out, t, dt, nullptr, ctx->stream);
 }
 
 dgsem_status dgsem_ssprk3_step(dgsem_ctx* ctx, double* u, double t, double dt) {
@@ -433,6 +457,96 @@ dgsem_status dgsem_ssprk3_steps(dgsem_ctx* ctx, double* u, double t0, double dt,
     dgsem_status st = dgsem_ssprk3_step(ctx, u, t0 + s * dt, dt);
     if (st != DGSEM_OK) return st;
   }
+  return DGSEM_OK;
+}
+
+dgsem_status dgsem_ssprk3_steps_host(dgsem_ctx* ctx, double* u_host, double t0,
+                                     double dt, int nsteps) {
+  if (!ctx || !u_host || nsteps < 0) return DGSEM_ERR_INVALID_ARG;
+  const size_t bytes = (size_t)ctx->state_len * sizeof(double);
+  cudaError_t e = cudaMemcpyAsync(ctx->staging, u_host, bytes,
+                                  cudaMemcpyHostToDevice, ctx->stream);
+  if (e != cudaSuccess) return DGSEM_ERR_CUDA;
+  dgsem_status st = dgsem_ssprk3_steps(ctx, ctx->staging, t0, dt, nsteps);
+  if (st != DGSEM_OK) return st;
+  e = cudaMemcpyAsync(u_host, ctx->staging, bytes, cudaMemcpyDeviceToHost,
+                      ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  return cuda_status(e);
+}
+
+struct dgsem_graph {
+  dgsem_ctx* ctx = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int nsteps = 0;
+  double dt = 0.0;
+};
+
+namespace {
+__global__ void set_clock_kernel(double* t_dev, double t) { *t_dev = t; }
+}  // namespace
+
+dgsem_status dgsem_graph_create(dgsem_ctx* ctx, double* u, double dt,
+                                int nsteps, dgsem_graph** out) {
+  if (!ctx || !u || !out || nsteps < 1) return DGSEM_ERR_INVALID_ARG;
+  *out = nullptr;
+  cudaStream_t cap;
+  if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess)
+    return DGSEM_ERR_CUDA;
+  dgsem_graph* g = new (std::nothrow) dgsem_graph();
+  if (!g) {
+    cudaStreamDestroy(cap);
+    return DGSEM_ERR_ALLOC;
+  }
+  g->ctx = ctx;
+  g->nsteps = nsteps;
+  g->dt = dt;
+  dgsem_status st = DGSEM_OK;
+  cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    for (int s = 0; s < nsteps && st == DGSEM_OK; ++s) {
+      const double toff = s * dt;
+      st = launch_stage(ctx, 1, nullptr, u, ctx->tmp1, toff, dt, ctx->tdev, cap);
+      if (st == DGSEM_OK)
+        st = launch_stage(ctx, 2, u, ctx->tmp1, ctx->tmp2, toff, dt, ctx->tdev, cap);
+      if (st == DGSEM_OK)
+        st = launch_stage(ctx, 3, u, ctx->tmp2, u, toff, dt, ctx->tdev, cap);
+    }
+    cudaError_t e2 = cudaStreamEndCapture(cap, &g->graph);
+    if (e2 != cudaSuccess && st == DGSEM_OK) st = DGSEM_ERR_CUDA;
+  } else {
+    st = DGSEM_ERR_CUDA;
+  }
+  if (st == DGSEM_OK &&
+      cudaGraphInstantiate(&g->exec, g->graph, 0) != cudaSuccess)
+    st = DGSEM_ERR_CUDA;
+  cudaStreamDestroy(cap);
+  if (st != DGSEM_OK) {
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    return st;
+  }
+  *out = g;
+  return DGSEM_OK;
+}
+
+dgsem_status dgsem_graph_launch(dgsem_graph* g, double t0) {
+  if (!g || !g->exec) return DGSEM_ERR_INVALID_ARG;
+  dgsem_ctx* ctx = g->ctx;
+  set_clock_kernel<<<1, 1, 0, ctx->stream>>>(ctx->tdev, t0);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaGraphLaunch(g->exec, ctx->stream);
+  ctx->launches += 1 + 3 * (int64_t)g->nsteps * ctx->engine->kernels_per_stage();
+  return cuda_status(e);
+}
+
+dgsem_status dgsem_graph_destroy(dgsem_graph* g) {
+  if (!g) return DGSEM_ERR_INVALID_ARG;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
   return DGSEM_OK;
 }
 

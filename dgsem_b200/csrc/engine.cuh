@@ -8,6 +8,7 @@
 
 #include <memory>
 
+#include "br1_kernel.cuh"
 #include "stage_kernel.cuh"
 #include "tables.hpp"
 
@@ -28,6 +29,7 @@ struct EngineConfig {
   BcParams bc;
   BasisTables basis;
   unsigned int* nonfinite;  // device flag
+  double* grad;             // Navier-Stokes lifted gradient [E][4][2][n^2]
 };
 
 class EngineBase {
@@ -36,15 +38,16 @@ class EngineBase {
   // out = a*u_n + b*u_in + c*RHS(u_in, t); alpha_out optional.
   virtual cudaError_t stage(const EngineConfig& cfg, const double* u_n,
                             const double* u_in, double* out, double a, double b,
-                            double c, double t, double* alpha_out,
-                            cudaStream_t s) = 0;
+                            double c, double t, const double* t_dev,
+                            double* alpha_out, cudaStream_t s) = 0;
+  virtual int kernels_per_stage() const = 0;
   virtual int elements_per_block() const = 0;
   virtual int threads_per_block() const = 0;
   virtual size_t smem_bytes() const = 0;
 };
 
 std::unique_ptr<EngineBase> make_engine(int ndims, int n, int vf, int sf,
-                                        bool hg);
+                                        bool hg, bool ns);
 
 template <int N>
 inline void fill_basis_const(const BasisTables& b, BasisConst<N>* out) {
@@ -69,24 +72,25 @@ struct LaunchShape {
   static constexpr int NT = ((EPB * NLINE + 31) / 32) * 32;
 };
 
-template <int DIM, int N, int VF, int SF, bool HG>
+template <int DIM, int N, int VF, int SF, bool HG, bool NS = false>
 class Engine final : public EngineBase {
  public:
   using L = LaunchShape<DIM, N>;
   static constexpr int EPB = L::EPB;
   static constexpr int NT = L::NT;
-  using Shape = StageShape<DIM, N, VF, SF, HG, EPB>;
+  using Shape = StageShape<DIM, N, VF, SF, HG, EPB, NS>;
+  static constexpr int GRAD_EPB = (128 / (N * N)) > 0 ? (128 / (N * N)) : 1;
 
   Engine() {
-    cudaFuncSetAttribute(stage_kernel<DIM, N, VF, SF, HG, EPB, NT>,
+    cudaFuncSetAttribute(stage_kernel<DIM, N, VF, SF, HG, EPB, NT, NS>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)Shape::smem_bytes);
   }
 
   cudaError_t stage(const EngineConfig& cfg, const double* u_n,
                     const double* u_in, double* out, double a, double b,
-                    double c, double t, double* alpha_out,
-                    cudaStream_t s) override {
+                    double c, double t, const double* t_dev,
+                    double* alpha_out, cudaStream_t s) override {
     StageArgs<N> args;
     args.u_in = u_in;
     args.u_n = u_n;
@@ -95,6 +99,7 @@ class Engine final : public EngineBase {
     args.b = b;
     args.c = c;
     args.t = t;
+    args.t_dev = t_dev;
     for (int i = 0; i < 3; ++i) {
       args.cells[i] = cfg.cells[i];
       args.periodic[i] = cfg.periodic[i];
@@ -109,17 +114,31 @@ class Engine final : public EngineBase {
     args.hg_s = cfg.hg_s;
     args.alpha_out = alpha_out;
     args.nonfinite = cfg.nonfinite;
-    args.grad = nullptr;
+    args.grad = cfg.grad;
     args.mu = cfg.mu;
     args.kappa = cfg.gamma / ((cfg.gamma - 1.0) * cfg.prandtl);
     args.tab = cfg.tab;
     args.bc = cfg.bc;
     fill_basis_const<N>(cfg.basis, &args.basis);
+    if constexpr (NS) {
+      GradArgs<N> ga;
+      ga.u = u_in;
+      ga.grad = cfg.grad;
+      for (int i = 0; i < 3; ++i) ga.cells[i] = cfg.cells[i];
+      ga.nelem = cfg.nelem;
+      ga.gamma = cfg.gamma;
+      ga.tab = cfg.tab;
+      ga.basis = args.basis;
+      const int64_t gblocks = (cfg.nelem + GRAD_EPB - 1) / GRAD_EPB;
+      br1_gradient_kernel<N, GRAD_EPB>
+          <<<(unsigned)gblocks, GRAD_EPB * N * N, 0, s>>>(ga);
+    }
     const int64_t blocks = (cfg.nelem + EPB - 1) / EPB;
-    stage_kernel<DIM, N, VF, SF, HG, EPB, NT>
+    stage_kernel<DIM, N, VF, SF, HG, EPB, NT, NS>
         <<<(unsigned)blocks, NT, Shape::smem_bytes, s>>>(args);
     return cudaGetLastError();
   }
+  int kernels_per_stage() const override { return NS ? 2 : 1; }
   int elements_per_block() const override { return EPB; }
   int threads_per_block() const override { return NT; }
   size_t smem_bytes() const override { return Shape::smem_bytes; }

@@ -74,7 +74,9 @@ struct StageArgs {
   const double* u_n;
   double* out;
   double a, b, c;  // out = a*u_n + b*u_in + c*du
-  double t;
+  double t;             // stage time when t_dev is null
+  const double* t_dev;  // optional device clock: stage time = *t_dev + t
+
   int64_t cells[3];
   int64_t nelem;
   int periodic[3];
@@ -182,7 +184,9 @@ __device__ __forceinline__ void reflect_state(const double* ui, const double* n,
 // Evaluated with explicitly rounded products and sums (no contraction) in
 // the reference's order, so alpha and the troubled-cell flag match.
 // ---------------------------------------------------------------------------
-template <int N>
+// PAD selects the padded shared-memory node layout (node j*N+i stored at
+// j*(N+1)+i); ND is the stride between variables.
+template <int N, bool PAD = false>
 __device__ double hg_alpha_2d(const double* us_el, int ND, const BasisConst<N>& B,
                               double threshold, double s, double alpha_min,
                               double alpha_max) {
@@ -191,7 +195,7 @@ __device__ double hg_alpha_2d(const double* us_el, int ND, const BasisConst<N>& 
   for (int j = 0; j < N; ++j)
 #pragma unroll
     for (int i = 0; i < N; ++i) {
-      const int node = j * N + i;
+      const int node = PAD ? j * (N + 1) + i : j * N + i;
       const double rho = us_el[0 * ND + node];
       const double u_vel = __ddiv_rn(us_el[1 * ND + node], rho);
       const double v_vel = __ddiv_rn(us_el[2 * ND + node], rho);
@@ -247,73 +251,165 @@ __device__ double hg_alpha_2d(const double* us_el, int ND, const BasisConst<N>& 
 // ---------------------------------------------------------------------------
 // The fused stage kernel
 // ---------------------------------------------------------------------------
-template <int DIM, int N, int VF, int SF, bool HG, int EPB>
+// Shared-memory node arrays are padded by one slot per N nodes
+// (pnode = node + node / N) so that the per-line strided accesses of the
+// volume phase fall on distinct banks.
+template <int N>
+__device__ __forceinline__ constexpr int padn(int node) {
+  return node + node / N;
+}
+
+template <int DIM, int N, int VF, int SF, bool HG, int EPB, bool NS = false>
 struct StageShape {
   static constexpr int NV = DIM + 2;
   static constexpr int ND = ipow(N, DIM);
+  static constexpr int NDP = ND + ND / N;  // padded node count
   static constexpr int NF = ipow(N, DIM - 1);
   static constexpr int NFACE = 2 * DIM;
   static constexpr int NLINE = DIM * NF;
-  static constexpr int NQ = DIM + 3;  // v[DIM], p, beta, kin
-  static constexpr int SM_U = EPB * NV * ND;
-  static constexpr int SM_P = EPB * NQ * ND;
+  // per node: v[DIM], p, beta, kin, sound speed, -1/J
+  static constexpr int NQ = DIM + 5;
+  static constexpr int Q_P = DIM, Q_BETA = DIM + 1, Q_KIN = DIM + 2, Q_A = DIM + 3,
+                       Q_MIJ = DIM + 4;
+  static constexpr int SM_U = EPB * NV * NDP;
+  static constexpr int SM_P = EPB * NQ * NDP;
   static constexpr int SM_F = EPB * NFACE * NV * NF;
-  static constexpr int SM_V = EPB * DIM * NV * ND;
+  static constexpr int SM_V = EPB * DIM * NV * NDP;
   static constexpr int SM_A = EPB;
+  static constexpr int SM_W = NS ? EPB * DIM * NV * NDP : 0;  // -F_v [el][dim][var][node]
+  // per element int info: ijk[3], eidx_other[3], neighbour[6] (-1 = boundary)
+  static constexpr int NI = 12;
   static constexpr size_t smem_bytes =
-      sizeof(double) * (SM_U + SM_P + SM_F + SM_V + SM_A);
+      sizeof(double) * (SM_U + SM_P + SM_F + SM_V + SM_A + SM_W) + sizeof(int) * EPB * NI;
 };
 
-template <int DIM, int N, int VF, int SF, bool HG, int EPB, int NT>
+// Navier-Stokes pieces used by the stage kernel (defined in br1_kernel.cuh).
+__device__ __forceinline__ void ns_gradient_variables(const double* u, double gamma,
+                                                      double* q);
+__device__ __forceinline__ void ns_neg_viscous_flux(const double* q, const double* gx,
+                                                    const double* gy, double mu,
+                                                    double kappa, int dim, double* f);
+
+template <int DIM, int N, int VF, int SF, bool HG, int EPB, int NT, bool NS = false>
 __global__ void __launch_bounds__(NT)
     stage_kernel(const StageArgs<N> p) {
-  using S = StageShape<DIM, N, VF, SF, HG, EPB>;
-  constexpr int NV = S::NV, ND = S::ND, NF = S::NF, NFACE = S::NFACE,
-                NLINE = S::NLINE, NQ = S::NQ;
+  using S = StageShape<DIM, N, VF, SF, HG, EPB, NS>;
+  static_assert(!NS || (DIM == 2 && !HG), "Navier-Stokes: 2D split form only");
+  static_assert(!HG || DIM == 2, "shock capturing: 2D only");
+  constexpr int NV = S::NV, ND = S::ND, NDP = S::NDP, NF = S::NF, NFACE = S::NFACE,
+                NLINE = S::NLINE, NQ = S::NQ, NI = S::NI;
   extern __shared__ double smem[];
-  double* us = smem;
-  double* pr = us + S::SM_U;
-  double* fs = pr + S::SM_P;
-  double* dv = fs + S::SM_F;
-  double* alpha_s = dv + S::SM_V;
+  double* us = smem;                 // [el][var][pnode]
+  double* pr = us + S::SM_U;         // [el][q][pnode]
+  double* fs = pr + S::SM_P;         // [el][face][var][fn]
+  double* dv = fs + S::SM_F;         // [el][dir][var][pnode]
+  double* alpha_s = dv + S::SM_V;    // [el]
+  double* wv = alpha_s + S::SM_A;    // [el][dim][var][pnode] (NS)
+  int* info = reinterpret_cast<int*>(wv + S::SM_W);
 
   const int tid = threadIdx.x;
-  const int64_t e0 = (int64_t)blockIdx.x * EPB;
-  if (e0 >= p.nelem) return;
-  const int ne = (int)min((int64_t)EPB, p.nelem - e0);
+  const int e0 = (int)blockIdx.x * EPB;
+  const int nelem = (int)p.nelem;
+  if (e0 >= nelem) return;
+  const int ne = min(EPB, nelem - e0);
   const double gamma = p.gamma;
+  const double t_stage = p.t_dev ? (*p.t_dev + p.t) : p.t;
+  const int c0 = (int)p.cells[0], c1 = (int)p.cells[1], c2 = (int)p.cells[2];
 
-  // ---- phase 0: load the contiguous u_in tile ---------------------------
-  {
-    const double2* src = reinterpret_cast<const double2*>(p.u_in + e0 * NV * ND);
-    double2* dst = reinterpret_cast<double2*>(us);
-    const int total = ne * NV * ND;
-    if ((total & 1) == 0) {
-      for (int idx = tid; idx < total / 2; idx += NT) dst[idx] = __ldg(src + idx);
+  // ---- phase 0: element info and the contiguous u_in tile ----------------
+  for (int el = tid; el < ne; el += NT) {
+    const int e = e0 + el;
+    int ijk[3];
+    ijk[0] = e % c0;
+    ijk[1] = DIM == 2 ? e / c0 : (e / c0) % c1;
+    ijk[2] = DIM == 2 ? 0 : e / (c0 * c1);
+    int* I = info + el * NI;
+    I[0] = ijk[0];
+    I[1] = ijk[1];
+    I[2] = ijk[2];
+    if (DIM == 2) {
+      I[3] = ijk[1];
+      I[4] = ijk[0];
+      I[5] = 0;
     } else {
-      for (int idx = tid; idx < total; idx += NT) us[idx] = __ldg(p.u_in + e0 * NV * ND + idx);
+      I[3] = ijk[1] + c1 * ijk[2];
+      I[4] = ijk[0] + c0 * ijk[2];
+      I[5] = ijk[0] + c0 * ijk[1];
+    }
+    const int cells[3] = {c0, c1, c2};
+#pragma unroll
+    for (int face = 0; face < NFACE; ++face) {
+      const int dir = face >> 1, side = face & 1;
+      int pos = ijk[dir] + (side ? 1 : -1);
+      int nbr = -1;
+      if (pos < 0 || pos >= cells[dir]) {
+        if (p.periodic[dir]) pos = (pos + cells[dir]) % cells[dir];
+        else pos = -1;
+      }
+      if (pos >= 0) {
+        int q[3] = {ijk[0], ijk[1], ijk[2]};
+        q[dir] = pos;
+        nbr = DIM == 2 ? q[0] + c0 * q[1] : q[0] + c0 * (q[1] + c1 * q[2]);
+      }
+      I[6 + face] = nbr;
+    }
+  }
+  {
+    const double* src = p.u_in + (int64_t)e0 * NV * ND;
+    for (int idx = tid; idx < ne * NV * ND; idx += NT) {
+      const int row = idx / ND, node = idx % ND;
+      us[row * NDP + padn<N>(node)] = __ldg(src + idx);
     }
   }
   __syncthreads();
 
-  // ---- phase 1: node primitives and HG alpha ----------------------------
+  // ---- phase 1: node primitives, sound speed, -1/J, HG alpha --------------
   for (int idx = tid; idx < ne * ND; idx += NT) {
     const int el = idx / ND, node = idx % ND;
+    const int pn = padn<N>(node);
     double u[NV];
 #pragma unroll
-    for (int q = 0; q < NV; ++q) u[q] = us[(el * NV + q) * ND + node];
+    for (int q = 0; q < NV; ++q) u[q] = us[(el * NV + q) * NDP + pn];
     const NodeState<DIM> s = prepare_node<DIM, VF>(u, gamma);
-    double* P = pr + el * NQ * ND + node;
+    double* P = pr + el * NQ * NDP + pn;
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) P[d * ND] = s.v[d];
-    P[DIM * ND] = s.p;
-    P[(DIM + 1) * ND] = s.beta;
-    P[(DIM + 2) * ND] = s.kin;
+    for (int d = 0; d < DIM; ++d) P[d * NDP] = s.v[d];
+    P[S::Q_P * NDP] = s.p;
+    P[S::Q_BETA * NDP] = s.beta;
+    P[S::Q_KIN * NDP] = s.kin;
+    P[S::Q_A * NDP] = sqrt(gamma * s.p / u[0]);
+    const int* I = info + el * NI;
+    const int in = node % N, jn = (node / N) % N, kn = DIM == 3 ? node / (N * N) : 0;
+    double jdet = __ldg(p.tab.jdiag[0] + I[0] * N + in);
+    if (DIM == 2) {
+      jdet = jdet * __ldg(p.tab.jdiag[1] + I[1] * N + jn);
+    } else {
+      jdet = jdet * (__ldg(p.tab.jdiag[1] + I[1] * N + jn) * __ldg(p.tab.jdiag[2] + I[2] * N + kn));
+    }
+    P[S::Q_MIJ * NDP] = -(1.0 / jdet);
+    if constexpr (NS) {
+      // -F_v at the node from the lifted gradient (parabolic_viscous.hpp:358-396)
+      double q[4], gx[4], gy[4];
+      ns_gradient_variables(u, gamma, q);
+      const double* G = p.grad + (int64_t)(e0 + el) * 4 * 2 * ND + node;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        gx[v] = __ldg(G + (v * 2 + 0) * ND);
+        gy[v] = __ldg(G + (v * 2 + 1) * ND);
+      }
+#pragma unroll
+      for (int d = 0; d < 2; ++d) {
+        double f[4];
+        ns_neg_viscous_flux(q, gx, gy, p.mu, p.kappa, d, f);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) wv[((el * 2 + d) * NV + v) * NDP + pn] = f[v];
+      }
+    }
   }
   if (HG) {
     for (int el = tid; el < ne; el += NT) {
-      const double a = hg_alpha_2d<N>(us + el * NV * ND, ND, p.basis, p.hg_threshold,
-                                      p.hg_s, p.alpha_min, p.alpha_max);
+      const double a = hg_alpha_2d<N, true>(us + el * NV * NDP, NDP, p.basis, p.hg_threshold,
+                                             p.hg_s, p.alpha_min, p.alpha_max);
       alpha_s[el] = a;
       if (p.alpha_out) p.alpha_out[e0 + el] = a;
     }
@@ -326,61 +422,101 @@ __global__ void __launch_bounds__(NT)
     const int face = (idx / NF) % NFACE;
     const int fn = idx % NF;
     const int dir = face >> 1, side = face & 1;
-    const int64_t e = e0 + el;
-    const ElemIdx<DIM> ei = elem_coords<DIM>(e, p.cells);
+    const int* I = info + el * NI;
     const int own_node = face_node<DIM, N>(dir, fn, side ? N - 1 : 0);
-    double uo[NV];
+    const int opn = padn<N>(own_node);
+    FaceState<DIM> so;
+    {
+      const double* P = pr + el * NQ * NDP + opn;
 #pragma unroll
-    for (int q = 0; q < NV; ++q) uo[q] = us[(el * NV + q) * ND + own_node];
-    const FaceState<DIM> so = prepare_face<DIM>(uo, gamma);
-    // neighbour along dir
-    ElemIdx<DIM> nb = ei;
-    const int64_t ncell = p.cells[dir];
-    const int64_t pos = ei.i[dir] + (side ? 1 : -1);
-    bool boundary = false;
-    if (pos < 0 || pos >= ncell) {
-      if (p.periodic[dir]) {
-        nb.i[dir] = (pos + ncell) % ncell;
-      } else {
-        boundary = true;
-      }
-    } else {
-      nb.i[dir] = pos;
+      for (int q = 0; q < NV; ++q) so.u[q] = us[(el * NV + q) * NDP + opn];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) so.v[d] = P[d * NDP];
+      so.p = P[S::Q_P * NDP];
+      so.a = P[S::Q_A * NDP];
     }
+    const int en = I[6 + face];
     double f[NV];
-    if (!boundary) {
-      const int64_t en = elem_linear<DIM>(nb, p.cells);
+    if (en >= 0) {
       const int nb_node = face_node<DIM, N>(dir, fn, side ? 0 : N - 1);
       double un[NV];
 #pragma unroll
-      for (int q = 0; q < NV; ++q) un[q] = __ldg(p.u_in + (en * NV + q) * ND + nb_node);
+      for (int q = 0; q < NV; ++q)
+        un[q] = __ldg(p.u_in + ((int64_t)en * NV + q) * ND + nb_node);
       const FaceState<DIM> sn = prepare_face<DIM>(un, gamma);
       // normal: Ja^dir of the element on the high side at its low-face node
-      const ElemIdx<DIM>& er = side ? nb : ei;
       const int r_node = face_node<DIM, N>(dir, fn, 0);
       double nrm[DIM];
 #pragma unroll
-      for (int c = 0; c < DIM; ++c)
-        nrm[c] = ja_at(p.tab.ja[dir][c], eidx_other<DIM>(er, c, p.cells), ND, r_node);
+      for (int c = 0; c < DIM; ++c) {
+        int eo;
+        if (side) {
+          // element-index over the axes != c of the neighbour: equal to ours
+          // unless c is the direction of the face
+          if (c == dir) {
+            eo = I[3 + c];
+          } else {
+            const int nq = (dir == 0) ? (en % c0)
+                         : (dir == 1) ? (DIM == 2 ? en / c0 : (en / c0) % c1)
+                                      : en / (c0 * c1);
+            if (DIM == 2) {
+              eo = nq;
+            } else {
+              const int ax0 = (c == 0) ? 1 : 0;         // first axis != c
+              const int ax1 = (c == 2) ? 1 : 2;         // second axis != c
+              const int i0 = (ax0 == dir) ? nq : I[ax0];
+              const int i1 = (ax1 == dir) ? nq : I[ax1];
+              eo = i0 + (ax0 == 0 ? c0 : c1) * i1;
+            }
+          }
+        } else {
+          eo = I[3 + c];
+        }
+        nrm[c] = ja_at(p.tab.ja[dir][c], eo, ND, r_node);
+      }
       if (side) {
         surface_flux<DIM, SF>(so, sn, nrm, gamma, f);
       } else {
         surface_flux<DIM, SF>(sn, so, nrm, gamma, f);
+      }
+      if constexpr (NS) {
+        // one-sided viscous interface flux: -F_v . n of the high-side
+        // (primary) element at its low-face node (parabolic_viscous.hpp:570-585);
+        // lifted with the same factors as the inviscid flux, so it is summed in.
+        double w[2][4];
+        if (side) {
+          double q[4], gx[4], gy[4];
+          ns_gradient_variables(un, gamma, q);
+          const double* G = p.grad + (int64_t)en * 4 * 2 * ND + nb_node;
+#pragma unroll
+          for (int v = 0; v < 4; ++v) {
+            gx[v] = __ldg(G + (v * 2 + 0) * ND);
+            gy[v] = __ldg(G + (v * 2 + 1) * ND);
+          }
+          ns_neg_viscous_flux(q, gx, gy, p.mu, p.kappa, 0, w[0]);
+          ns_neg_viscous_flux(q, gx, gy, p.mu, p.kappa, 1, w[1]);
+        } else {
+#pragma unroll
+          for (int d = 0; d < 2; ++d)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) w[d][v] = wv[((el * 2 + d) * NV + v) * NDP + opn];
+        }
+#pragma unroll
+        for (int v = 0; v < 4; ++v) f[v] += w[0][v] * nrm[0] + w[1][v] * nrm[1];
       }
     } else {
       // boundary_helper.hpp:93-146: own metric at the boundary node;
       // inner state is the left state on high faces.
       double nrm[DIM];
 #pragma unroll
-      for (int c = 0; c < DIM; ++c)
-        nrm[c] = ja_at(p.tab.ja[dir][c], eidx_other<DIM>(ei, c, p.cells), ND, own_node);
+      for (int c = 0; c < DIM; ++c) nrm[c] = ja_at(p.tab.ja[dir][c], I[3 + c], ND, own_node);
       double ub[NV];
       const int kind = p.bc.kind[face];
       if (DIM == 2) {
-        const double x = __ldg(p.tab.coord[0] + ei.i[0] * N + (own_node % N));
-        const double y = __ldg(p.tab.coord[1] + ei.i[1] * N + (own_node / N));
+        const double x = __ldg(p.tab.coord[0] + I[0] * N + (own_node % N));
+        const double y = __ldg(p.tab.coord[1] + I[1] * N + (own_node / N));
         if (kind == BC_DIRICHLET_DMR) {
-          dmr_state(p.bc, x, y, p.t, ub);
+          dmr_state(p.bc, x, y, t_stage, ub);
         } else if (kind == BC_DIRICHLET_CONST) {
 #pragma unroll
           for (int q = 0; q < NV; ++q) ub[q] = p.bc.state[q];
@@ -391,13 +527,13 @@ __global__ void __launch_bounds__(NT)
             double acc = 0.0;
 #pragma unroll
             for (int m = 0; m < N; ++m)
-              acc += us[(el * NV + q) * ND + face_node<DIM, N>(dir, fn, m)];
+              acc += us[(el * NV + q) * NDP + padn<N>(face_node<DIM, N>(dir, fn, m))];
             ub[q] = acc / (double)N;
           }
         } else if (kind == BC_MIXED_DMR_WALL && x < 1.0 / 6.0) {
-          dmr_state(p.bc, x, y, p.t, ub);
+          dmr_state(p.bc, x, y, t_stage, ub);
         } else {  // slip wall / wall branch of the mixed BC
-          reflect_state(uo, nrm, ub);
+          reflect_state(so.u, nrm, ub);
         }
       }
       const FaceState<DIM> sb = prepare_face<DIM>(ub, gamma);
@@ -416,14 +552,13 @@ __global__ void __launch_bounds__(NT)
     const int el = idx / NLINE;
     const int dir = (idx % NLINE) / NF;
     const int line = idx % NF;
-    const int64_t e = e0 + el;
-    const ElemIdx<DIM> ei = elem_coords<DIM>(e, p.cells);
-    const double* U = us + el * NV * ND;
-    const double* P = pr + el * NQ * ND;
+    const int* I = info + el * NI;
+    const double* U = us + el * NV * NDP;
+    const double* P = pr + el * NQ * NDP;
     double ja[N][DIM];
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
-      const double* tab = p.tab.ja[dir][c] + eidx_other<DIM>(ei, c, p.cells) * ND;
+      const double* tab = p.tab.ja[dir][c] + (int64_t)I[3 + c] * ND;
 #pragma unroll
       for (int m = 0; m < N; ++m) ja[m][c] = __ldg(tab + line_node<DIM, N>(dir, line, m));
     }
@@ -434,24 +569,24 @@ __global__ void __launch_bounds__(NT)
       for (int q = 0; q < NV; ++q) acc[m][q] = 0.0;
 #pragma unroll
     for (int i = 0; i < N; ++i) {
-      const int ni = line_node<DIM, N>(dir, line, i);
+      const int ni = padn<N>(line_node<DIM, N>(dir, line, i));
       NodeState<DIM> Li;
       Li.rho = U[ni];
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) Li.v[d] = P[d * ND + ni];
-      Li.p = P[DIM * ND + ni];
-      Li.beta = P[(DIM + 1) * ND + ni];
-      Li.kin = P[(DIM + 2) * ND + ni];
+      for (int d = 0; d < DIM; ++d) Li.v[d] = P[d * NDP + ni];
+      Li.p = P[S::Q_P * NDP + ni];
+      Li.beta = P[S::Q_BETA * NDP + ni];
+      Li.kin = P[S::Q_KIN * NDP + ni];
 #pragma unroll
       for (int k = i + 1; k < N; ++k) {
-        const int nk = line_node<DIM, N>(dir, line, k);
+        const int nk = padn<N>(line_node<DIM, N>(dir, line, k));
         NodeState<DIM> Rk;
         Rk.rho = U[nk];
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) Rk.v[d] = P[d * ND + nk];
-        Rk.p = P[DIM * ND + nk];
-        Rk.beta = P[(DIM + 1) * ND + nk];
-        Rk.kin = P[(DIM + 2) * ND + nk];
+        for (int d = 0; d < DIM; ++d) Rk.v[d] = P[d * NDP + nk];
+        Rk.p = P[S::Q_P * NDP + nk];
+        Rk.beta = P[S::Q_BETA * NDP + nk];
+        Rk.kin = P[S::Q_KIN * NDP + nk];
         double nrm[DIM];
 #pragma unroll
         for (int c = 0; c < DIM; ++c) nrm[c] = 0.5 * (ja[i][c] + ja[k][c]);
@@ -466,6 +601,25 @@ __global__ void __launch_bounds__(NT)
         }
       }
     }
+    if constexpr (NS) {
+      // viscous weak-form volume term along the line with Dhat on the
+      // contravariant flux Ja^dir . (-F_v) (parabolic_viscous.hpp:418-466)
+      double fc[N][NV];
+#pragma unroll
+      for (int m = 0; m < N; ++m) {
+        const int nm = padn<N>(line_node<DIM, N>(dir, line, m));
+#pragma unroll
+        for (int q = 0; q < NV; ++q)
+          fc[m][q] = ja[m][0] * wv[((el * 2 + 0) * NV + q) * NDP + nm] +
+                     ja[m][1] * wv[((el * 2 + 1) * NV + q) * NDP + nm];
+      }
+#pragma unroll
+      for (int m = 0; m < N; ++m)
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+#pragma unroll
+          for (int q = 0; q < NV; ++q) acc[m][q] += p.basis.Dhat[m][k] * fc[k][q];
+    }
     if (HG) {
       const double alpha = alpha_s[el];
       if (fabs(alpha - 0.0) > p.atol) {
@@ -476,26 +630,25 @@ __global__ void __launch_bounds__(NT)
 #pragma unroll
           for (int q = 0; q < NV; ++q) acc[m][q] *= one_m;
         // volume_flux.hpp:457-509: LLF on subcell normals along the line
-        FaceState<DIM> sl;
-        {
-          double uu[NV];
-          const int n0 = line_node<DIM, N>(dir, line, 0);
+        auto node_state = [&](int m) {
+          const int nm = padn<N>(line_node<DIM, N>(dir, line, m));
+          FaceState<DIM> st;
 #pragma unroll
-          for (int q = 0; q < NV; ++q) uu[q] = U[q * ND + n0];
-          sl = prepare_face<DIM>(uu, gamma);
-        }
+          for (int q = 0; q < NV; ++q) st.u[q] = U[q * NDP + nm];
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) st.v[d] = P[d * NDP + nm];
+          st.p = P[S::Q_P * NDP + nm];
+          st.a = P[S::Q_A * NDP + nm];
+          return st;
+        };
+        FaceState<DIM> sl = node_state(0);
 #pragma unroll
         for (int fi = 1; fi < N; ++fi) {
-          double uu[NV];
-          const int nr = line_node<DIM, N>(dir, line, fi);
-#pragma unroll
-          for (int q = 0; q < NV; ++q) uu[q] = U[q * ND + nr];
-          const FaceState<DIM> sr = prepare_face<DIM>(uu, gamma);
+          const FaceState<DIM> sr = node_state(fi);
           double nrm[DIM];
 #pragma unroll
           for (int c = 0; c < DIM; ++c)
-            nrm[c] = __ldg(p.tab.fv[dir][c] +
-                           eidx_other<DIM>(ei, c, p.cells) * (N - 1) * N + (fi - 1) * N + line);
+            nrm[c] = __ldg(p.tab.fv[dir][c] + (int64_t)I[3 + c] * (N - 1) * N + (fi - 1) * N + line);
           double f[NV];
           llf_flux<DIM>(sl, sr, nrm, f);
           const double wl = alpha * p.basis.inv_w[fi - 1];
@@ -509,27 +662,27 @@ __global__ void __launch_bounds__(NT)
         }
       }
     }
-    double* V = dv + (el * DIM + dir) * NV * ND;
+    double* V = dv + (el * DIM + dir) * NV * NDP;
 #pragma unroll
     for (int m = 0; m < N; ++m) {
-      const int nm = line_node<DIM, N>(dir, line, m);
+      const int nm = padn<N>(line_node<DIM, N>(dir, line, m));
 #pragma unroll
-      for (int q = 0; q < NV; ++q) V[q * ND + nm] = acc[m][q];
+      for (int q = 0; q < NV; ++q) V[q * NDP + nm] = acc[m][q];
     }
   }
   __syncthreads();
 
   // ---- phase 3: lift, -1/J, SSPRK3 combination, store ---------------------
   bool bad = false;
+  const int64_t gbase = (int64_t)e0 * NV * ND;
   for (int idx = tid; idx < ne * NV * ND; idx += NT) {
     const int el = idx / (NV * ND);
     const int q = (idx / ND) % NV;
     const int node = idx % ND;
-    const int64_t e = e0 + el;
-    const ElemIdx<DIM> ei = elem_coords<DIM>(e, p.cells);
+    const int pn = padn<N>(node);
     double du = 0.0;
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) du += dv[((el * DIM + d) * NV + q) * ND + node];
+    for (int d = 0; d < DIM; ++d) du += dv[((el * DIM + d) * NV + q) * NDP + pn];
     const int in = node % N;
     const int jn = (node / N) % N;
     const int kn = (DIM == 3) ? node / (N * N) : 0;
@@ -546,19 +699,12 @@ __global__ void __launch_bounds__(NT)
       if (pos[d] == 0) du -= fs[((el * NFACE + 2 * d) * NV + q) * NF + fn] * p.basis.lhat_l0;
       if (pos[d] == N - 1) du += fs[((el * NFACE + 2 * d + 1) * NV + q) * NF + fn] * p.basis.lhat_rN;
     }
-    double jdet = __ldg(p.tab.jdiag[0] + ei.i[0] * N + in);
-    if (DIM == 2) {
-      jdet = jdet * __ldg(p.tab.jdiag[1] + ei.i[1] * N + jn);
-    } else {
-      jdet = jdet * (__ldg(p.tab.jdiag[1] + ei.i[1] * N + jn) *
-                     __ldg(p.tab.jdiag[2] + ei.i[2] * N + kn));
-    }
-    du = du * (-(1.0 / jdet));
+    du = du * pr[(el * NQ + S::Q_MIJ) * NDP + pn];
     double val = p.c * du;
-    if (p.b != 0.0) val = p.b * us[idx] + val;
-    if (p.a != 0.0) val = p.a * __ldg(p.u_n + e0 * NV * ND + idx) + val;
+    if (p.b != 0.0) val = p.b * us[(el * NV + q) * NDP + pn] + val;
+    if (p.a != 0.0) val = p.a * p.u_n[gbase + idx] + val;
     bad |= !isfinite(val);
-    p.out[e0 * NV * ND + idx] = val;
+    p.out[gbase + idx] = val;
   }
   if (bad) atomicOr(p.nonfinite, 1u);
 }

@@ -31,7 +31,12 @@ def combos():
     for n in range(2, 6):
         for vf in range(3):
             out.add((3, n, vf, 0, 0))
-    return sorted(out)
+    return sorted((d, n, vf, sf, hg, 0) for (d, n, vf, sf, hg) in out) + ns_combos()
+
+
+def ns_combos():
+    # 2D Navier-Stokes (BR1, periodic): n in 2..8, the three volume fluxes, LLF.
+    return sorted((2, n, vf, 0, 0, 1) for n in range(2, 9) for vf in range(3))
 
 
 def generate() -> list[str]:
@@ -45,10 +50,10 @@ def generate() -> list[str]:
         path = os.path.join(GEN, f"engines_{d}d_n{n}.cu")
         lines = [f"// Generated by gen_engines.py: Engine instantiations, {d}D, n = {n}.",
                  '#include "../engine.cuh"', "namespace dgsem {"]
-        for (_, _, vf, sf, hg) in items:
-            lines.append(f"std::unique_ptr<EngineBase> create_engine_{d}_{n}_{vf}_{sf}_{hg}() {{")
+        for (_, _, vf, sf, hg, ns) in items:
+            lines.append(f"std::unique_ptr<EngineBase> create_engine_{d}_{n}_{vf}_{sf}_{hg}_{ns}() {{")
             lines.append(f"  return std::make_unique<Engine<{d}, {n}, {vf}, {sf}, "
-                         f"{'true' if hg else 'false'}>>();")
+                         f"{'true' if hg else 'false'}, {'true' if ns else 'false'}>>();")
             lines.append("}")
         lines.append("}  // namespace dgsem")
         _write_if_changed(path, "\n".join(lines) + "\n")
@@ -56,13 +61,14 @@ def generate() -> list[str]:
     path = os.path.join(GEN, "engine_factory.cu")
     lines = ["// Generated by gen_engines.py: runtime scheme -> Engine instantiation.",
              '#include "../engine.cuh"', "namespace dgsem {"]
-    for (d, n, vf, sf, hg) in cs:
-        lines.append(f"std::unique_ptr<EngineBase> create_engine_{d}_{n}_{vf}_{sf}_{hg}();")
-    lines.append("std::unique_ptr<EngineBase> make_engine(int ndims, int n, int vf, int sf, bool hg) {")
-    lines.append("  const int h = hg ? 1 : 0;")
-    for (d, n, vf, sf, hg) in cs:
-        lines.append(f"  if (ndims == {d} && n == {n} && vf == {vf} && sf == {sf} && h == {hg})"
-                     f" return create_engine_{d}_{n}_{vf}_{sf}_{hg}();")
+    for (d, n, vf, sf, hg, ns) in cs:
+        lines.append(f"std::unique_ptr<EngineBase> create_engine_{d}_{n}_{vf}_{sf}_{hg}_{ns}();")
+    lines.append("std::unique_ptr<EngineBase> make_engine(int ndims, int n, int vf, int sf, bool hg,"
+                 " bool ns) {")
+    lines.append("  const int h = hg ? 1 : 0, v = ns ? 1 : 0;")
+    for (d, n, vf, sf, hg, ns) in cs:
+        lines.append(f"  if (ndims == {d} && n == {n} && vf == {vf} && sf == {sf} && h == {hg}"
+                     f" && v == {ns}) return create_engine_{d}_{n}_{vf}_{sf}_{hg}_{ns}();")
     lines.append("  return nullptr;")
     lines.append("}")
     lines.append("}  // namespace dgsem")

@@ -160,6 +160,23 @@ dgsem_status dgsem_ssprk3_step(dgsem_ctx* ctx, double* u, double t, double dt);
 dgsem_status dgsem_ssprk3_steps(dgsem_ctx* ctx, double* u, double t0,
                                 double dt, int nsteps);
 
+/* nsteps SSPRK3 steps on a HOST array (the reference's host-side view of
+ * the state): copies u_host to the device, steps, copies back and
+ * synchronises.  u_host should be pinned for full copy bandwidth. */
+dgsem_status dgsem_ssprk3_steps_host(dgsem_ctx* ctx, double* u_host, double t0,
+                                     double dt, int nsteps);
+
+/* CUDA graph of nsteps SSPRK3 steps on the device state u (3*nsteps fused
+ * stage kernels).  dgsem_graph_launch(g, t0) replays it on the context's
+ * stream starting at time t0 (stage times read from a device clock, so
+ * time-dependent boundary states stay correct).  The graph keeps pointers to
+ * u and to the context's temporaries. */
+typedef struct dgsem_graph dgsem_graph;
+dgsem_status dgsem_graph_create(dgsem_ctx* ctx, double* u, double dt,
+                                int nsteps, dgsem_graph** out);
+dgsem_status dgsem_graph_launch(dgsem_graph* g, double t0);
+dgsem_status dgsem_graph_destroy(dgsem_graph* g);
+
 /* Hennemann-Gassner blending factor per element and troubled-cell flag
  * (alpha > max(100 eps, eps^0.75), volume_flux.hpp:772-773).  Either output
  * may be NULL. */

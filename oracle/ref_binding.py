@@ -42,6 +42,8 @@ class _Case(ctypes.Structure):
         ("prandtl", ctypes.c_double),
         ("alpha_max", ctypes.c_double),
         ("alpha_min", ctypes.c_double),
+        ("volume_flux", ctypes.c_int),
+        ("surface_flux", ctypes.c_int),
     ]
 
 
@@ -112,6 +114,8 @@ class RefCase:
     prandtl: float = 0.72
     alpha_max: float = 0.5
     alpha_min: float = 0.001
+    volume_flux: int = 0    # 0 Chandrashekar, 1 Ranocha (plugin), 2 Kennedy-Gruber (plugin)
+    surface_flux: int = 0   # 0 Lax-Friedrichs, 1 HLLC 2D (plugin)
     _h: int = field(default=0, repr=False)
 
     def __post_init__(self):
@@ -128,6 +132,8 @@ class RefCase:
         c.prandtl = self.prandtl
         c.alpha_max = self.alpha_max
         c.alpha_min = self.alpha_min
+        c.volume_flux = self.volume_flux
+        c.surface_flux = self.surface_flux
         self._c = c
         self._h = lib().dgsem_ref_create(ctypes.byref(c))
         if not self._h:

@@ -56,6 +56,8 @@ typedef struct {
   double prandtl;
   double alpha_max;
   double alpha_min;
+  int volume_flux;   // 0 Chandrashekar (reference), 1 Ranocha, 2 Kennedy-Gruber
+  int surface_flux;  // 0 LaxFriedrichs (reference), 1 HLLC (2D)
 } dgsem_ref_case;
 }
 
@@ -95,6 +97,152 @@ struct DmrBottomInflow {
   }
 };
 
+// ---------------------------------------------------------------------------
+// Two-point / surface fluxes the reference does not ship, written as plugins
+// with the reference's flux signature numerical_flux(eq, uL, uR, normal)
+// (base/numerical_flux.hpp:436-500) so they run inside the reference's own
+// VolumeIntegralSplitForm / InterfaceHelper / boundary assembly.
+//   Ranocha: J. Sci. Comput. 76 (2018) / (2020); Kennedy & Gruber: JCP 227
+//   (2008); HLLC: the reference's 1D HLLC (numerical_flux.hpp:283-378) in the
+//   face-normal frame with passive tangential momentum (Toro, ch. 10).
+// ---------------------------------------------------------------------------
+template <class Eq>
+struct PluginTraits {
+  static constexpr std::size_t D = Eq::NDIMS;
+  static constexpr std::size_t V = Eq::NVARS;
+};
+
+template <class Eq>
+void prim_of(const Eq& eq, const std::array<T, Eq::NVARS>& u, T& rho,
+             std::array<T, Eq::NDIMS>& v, T& p) {
+  constexpr std::size_t D = Eq::NDIMS;
+  rho = u[0];
+  T sq = 0;
+  for (std::size_t d = 0; d < D; ++d) {
+    v[d] = u[1 + d] / rho;
+    sq += v[d] * v[d];
+  }
+  p = (eq.get_gamma() - T(1)) * (u[D + 1] - T(0.5) * rho * sq);
+}
+
+template <class Eq>
+struct KennedyGruberPlugin {
+  static std::array<T, Eq::NVARS> numerical_flux(
+      const Eq& eq, const std::array<T, Eq::NVARS>& uL,
+      const std::array<T, Eq::NVARS>& uR, const std::array<T, Eq::NDIMS>& n) {
+    constexpr std::size_t D = Eq::NDIMS;
+    T rL, rR, pL, pR;
+    std::array<T, D> vL, vR;
+    prim_of(eq, uL, rL, vL, pL);
+    prim_of(eq, uR, rR, vR, pR);
+    const T rho_avg = T(0.5) * (rL + rR);
+    const T e_avg = T(0.5) * (uL[D + 1] / rL + uR[D + 1] / rR);
+    const T p_avg = T(0.5) * (pL + pR);
+    std::array<T, D> va;
+    T vn = 0;
+    for (std::size_t d = 0; d < D; ++d) {
+      va[d] = T(0.5) * (vL[d] + vR[d]);
+      vn += va[d] * n[d];
+    }
+    std::array<T, Eq::NVARS> f{};
+    f[0] = rho_avg * vn;
+    for (std::size_t d = 0; d < D; ++d) f[1 + d] = f[0] * va[d] + p_avg * n[d];
+    f[D + 1] = (rho_avg * e_avg + p_avg) * vn;
+    return f;
+  }
+};
+
+template <class Eq>
+struct RanochaPlugin {
+  static T inv_ln_mean(T x, T y) {
+    const T num = x * (x - T(2) * y) + y * y;
+    const T den = x * (x + T(2) * y) + y * y;
+    const T f2 = num / den;
+    if (f2 < T(1.0e-4)) {
+      const T poly = T(2) + f2 * (T(2.0 / 3.0) + f2 * (T(2.0 / 5.0) + f2 * T(2.0 / 7.0)));
+      return poly / (x + y);
+    }
+    return std::log(y / x) / (y - x);
+  }
+  static std::array<T, Eq::NVARS> numerical_flux(
+      const Eq& eq, const std::array<T, Eq::NVARS>& uL,
+      const std::array<T, Eq::NVARS>& uR, const std::array<T, Eq::NDIMS>& n) {
+    constexpr std::size_t D = Eq::NDIMS;
+    T rL, rR, pL, pR;
+    std::array<T, D> vL, vR;
+    prim_of(eq, uL, rL, vL, pL);
+    prim_of(eq, uR, rR, vR, pR);
+    T vnL = 0, vnR = 0, vLvR = 0;
+    for (std::size_t d = 0; d < D; ++d) {
+      vnL += vL[d] * n[d];
+      vnR += vR[d] * n[d];
+      vLvR += vL[d] * vR[d];
+    }
+    const T rho_mean = DGSEM::ln_mean(rL, rR);
+    const T inv_rho_p_mean = pL * pR * inv_ln_mean(rL * pR, rR * pL);
+    const T p_avg = T(0.5) * (pL + pR);
+    std::array<T, Eq::NVARS> f{};
+    f[0] = rho_mean * T(0.5) * (vnL + vnR);
+    for (std::size_t d = 0; d < D; ++d)
+      f[1 + d] = f[0] * (T(0.5) * (vL[d] + vR[d])) + p_avg * n[d];
+    f[D + 1] = f[0] * (T(0.5) * vLvR + inv_rho_p_mean / (eq.get_gamma() - T(1))) +
+               T(0.5) * (pL * vnR + pR * vnL);
+    return f;
+  }
+};
+
+struct HLLC2DPlugin {
+  using Eq = DGSEM::equations::CompressibleEuler2D<T>;
+  static std::array<T, 4> numerical_flux(const Eq& eq, const std::array<T, 4>& uL,
+                                         const std::array<T, 4>& uR,
+                                         const std::array<T, 2>& n) {
+    const T g = eq.get_gamma();
+    const T nn = std::sqrt(n[0] * n[0] + n[1] * n[1]);
+    const T nx = n[0] / nn, ny = n[1] / nn;
+    const T rL = uL[0], rR = uR[0];
+    const T mnL = uL[1] * nx + uL[2] * ny, mtL = -uL[1] * ny + uL[2] * nx;
+    const T mnR = uR[1] * nx + uR[2] * ny, mtR = -uR[1] * ny + uR[2] * nx;
+    const T EL = uL[3], ER = uR[3];
+    const T vL = mnL / rL, vR = mnR / rR, wL = mtL / rL, wR = mtR / rR;
+    const T pL = (g - T(1)) * (EL - T(0.5) * rL * (vL * vL + wL * wL));
+    const T pR = (g - T(1)) * (ER - T(0.5) * rR * (vR * vR + wR * wR));
+    const T cL = std::sqrt(g * pL / rL), cR = std::sqrt(g * pR / rR);
+    const T srL = std::sqrt(rL), srR = std::sqrt(rR), ss = srL + srR;
+    const T v_roe = (srL * vL + srR * vR) / ss;
+    const T w_roe = (srL * wL + srR * wR) / ss;
+    const T ek = T(0.5) * (v_roe * v_roe + w_roe * w_roe);
+    const T H_roe = (srL * ((EL + pL) / rL) + srR * ((ER + pR) / rR)) / ss;
+    const T c_roe = std::sqrt((g - T(1)) * (H_roe - ek));
+    const T SL = std::min(vL - cL, v_roe - c_roe);
+    const T SR = std::max(vR + cR, v_roe + c_roe);
+    T q[4];
+    if (SL >= 0) {
+      q[0] = mnL; q[1] = mnL * vL + pL; q[2] = mnL * wL; q[3] = vL * (EL + pL);
+    } else if (SR <= 0) {
+      q[0] = mnR; q[1] = mnR * vR + pR; q[2] = mnR * wR; q[3] = vR * (ER + pR);
+    } else {
+      const T sMuL = SL - vL, sMuR = SR - vR;
+      const T SS = (pR - pL + rL * vL * sMuL - rR * vR * sMuR) / (rL * sMuL - rR * sMuR);
+      if (SS >= 0) {
+        const T dS = rL * sMuL / (SL - SS);
+        const T eS = EL / rL + (SS - vL) * (SS + pL / (rL * sMuL));
+        q[0] = mnL + SL * (dS - rL);
+        q[1] = (mnL * vL + pL) + SL * (dS * SS - mnL);
+        q[2] = mnL * wL + SL * (dS * wL - mtL);
+        q[3] = vL * (EL + pL) + SL * (dS * eS - EL);
+      } else {
+        const T dS = rR * sMuR / (SR - SS);
+        const T eS = ER / rR + (SS - vR) * (SS + pR / (rR * sMuR));
+        q[0] = mnR + SR * (dS - rR);
+        q[1] = (mnR * vR + pR) + SR * (dS * SS - mnR);
+        q[2] = mnR * wR + SR * (dS * wR - mtR);
+        q[3] = vR * (ER + pR) + SR * (dS * eS - ER);
+      }
+    }
+    return {q[0] * nn, (q[1] * nx - q[2] * ny) * nn, (q[1] * ny + q[2] * nx) * nn, q[3] * nn};
+  }
+};
+
 class RefCaseBase {
  public:
   virtual ~RefCaseBase() = default;
@@ -106,14 +254,13 @@ class RefCaseBase {
 };
 
 template <class Eq, std::size_t N, class VolumeFlux, class Boundaries,
-          std::size_t D>
+          std::size_t D, class SurfaceFlux = DGSEM::LaxFriedrichsFlux<Eq>>
 class RefCase final : public RefCaseBase {
  public:
   using Basis = DGSEM::Basis::LobattoLegendreBasis<T, N>;
   using Mesh = DGSEM::StructuredMesh<T, D>;
-  using Solver = DGSEM::StructuredSolver<Eq, Basis, VolumeFlux,
-                                         DGSEM::LaxFriedrichsFlux<Eq>, Mesh,
-                                         Boundaries>;
+  using Solver = DGSEM::StructuredSolver<Eq, Basis, VolumeFlux, SurfaceFlux,
+                                         Mesh, Boundaries>;
   using Sol = DGSEM::Solution<Mesh, Basis, Eq>;
 
   RefCase(const dgsem_ref_case& c, const Eq& eq, const Boundaries& bcs,
@@ -224,8 +371,16 @@ RefCaseBase* make_case_n(const dgsem_ref_case& c) {
   using P = DGSEM::PeriodicBC;
   switch (c.kind) {
     case REF_EULER2D_PERIODIC_SPLIT: {
-      using VF = DGSEM::VolumeIntegralSplitForm<Basis, E2, DGSEM::ChandrashekarFlux>;
       auto b = DGSEM::BoundarySet(P{}, P{}, P{}, P{});
+      if (c.volume_flux == 1) {
+        using VF = DGSEM::VolumeIntegralSplitForm<Basis, E2, RanochaPlugin>;
+        return new RefCase<E2, N, VF, decltype(b), 2>(c, E2{c.gamma}, b, true);
+      }
+      if (c.volume_flux == 2) {
+        using VF = DGSEM::VolumeIntegralSplitForm<Basis, E2, KennedyGruberPlugin>;
+        return new RefCase<E2, N, VF, decltype(b), 2>(c, E2{c.gamma}, b, true);
+      }
+      using VF = DGSEM::VolumeIntegralSplitForm<Basis, E2, DGSEM::ChandrashekarFlux>;
       return new RefCase<E2, N, VF, decltype(b), 2>(c, E2{c.gamma}, b, true);
     }
     case REF_EULER2D_PERIODIC_HG: {
@@ -233,6 +388,8 @@ RefCaseBase* make_case_n(const dgsem_ref_case& c) {
           Basis, E2, DGSEM::ChandrashekarFlux, DGSEM::LaxFriedrichsFlux,
           DGSEM::HGIndicator<Basis, E2>>;
       auto b = DGSEM::BoundarySet(P{}, P{}, P{}, P{});
+      if (c.surface_flux == 1)
+        return new RefCase<E2, N, VF, decltype(b), 2, HLLC2DPlugin>(c, E2{c.gamma}, b, true);
       return new RefCase<E2, N, VF, decltype(b), 2>(c, E2{c.gamma}, b, true);
     }
     case REF_EULER2D_DMR_HG: {
@@ -244,11 +401,21 @@ RefCaseBase* make_case_n(const dgsem_ref_case& c) {
           DGSEM::DirichletBC(inflow), DGSEM::OutflowBC{},
           DGSEM::MixedDirichletSlipWallBC(inflow, DmrBottomInflow{}),
           DGSEM::DirichletBC(inflow));
+      if (c.surface_flux == 1)
+        return new RefCase<E2, N, VF, decltype(b), 2, HLLC2DPlugin>(c, E2{c.gamma}, b, false);
       return new RefCase<E2, N, VF, decltype(b), 2>(c, E2{c.gamma}, b, false);
     }
     case REF_EULER3D_PERIODIC_SPLIT: {
-      using VF = DGSEM::VolumeIntegralSplitForm<Basis, E3, DGSEM::ChandrashekarFlux>;
       auto b = DGSEM::BoundarySet(P{}, P{}, P{}, P{}, P{}, P{});
+      if (c.volume_flux == 1) {
+        using VF = DGSEM::VolumeIntegralSplitForm<Basis, E3, RanochaPlugin>;
+        return new RefCase<E3, N, VF, decltype(b), 3>(c, E3{c.gamma}, b, true);
+      }
+      if (c.volume_flux == 2) {
+        using VF = DGSEM::VolumeIntegralSplitForm<Basis, E3, KennedyGruberPlugin>;
+        return new RefCase<E3, N, VF, decltype(b), 3>(c, E3{c.gamma}, b, true);
+      }
+      using VF = DGSEM::VolumeIntegralSplitForm<Basis, E3, DGSEM::ChandrashekarFlux>;
       return new RefCase<E3, N, VF, decltype(b), 3>(c, E3{c.gamma}, b, true);
     }
     case REF_EULER3D_PERIODIC_HG: {

@@ -51,4 +51,6 @@ CASES = {
                 right=(2 * math.pi,) * 3, ic="tgv3d"),
     "vortex_n6": dict(ndims=2, polydeg=5, cells=(5, 7), left=(-5.0, -5.0), right=(5.0, 5.0),
                       ic="vortex"),
+    "ns": dict(ndims=2, polydeg=4, cells=(6, 6), left=(0.0, 0.0), right=(2 * math.pi,) * 2,
+               ic="tgv2d", viscous=True, mu=1.0e-3, prandtl=0.72, noise=1.0e-3),
 }

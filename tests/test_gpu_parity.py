@@ -20,11 +20,12 @@ VF = {"chandrashekar": "ChandrashekarFlux", "ranocha": "RanochaFlux",
 SF = {"llf": "LaxFriedrichsFlux", "hllc": "HLLCFlux"}
 REF_KIND = {("kh", False): rb.EULER2D_PERIODIC_SPLIT, ("kh", True): rb.EULER2D_PERIODIC_HG,
             ("dmr", True): rb.EULER2D_DMR_HG, ("tgv3d", False): rb.EULER3D_PERIODIC_SPLIT,
-            ("vortex", False): rb.EULER2D_PERIODIC_SPLIT}
+            ("vortex", False): rb.EULER2D_PERIODIC_SPLIT, ("tgv2d", False): rb.NS2D_PERIODIC_SPLIT}
 
 
 def make_oracle(case: dict, volume_flux="chandrashekar", surface_flux="llf"):
     kw = {k: v for k, v in case.items() if k not in ("ic", "noise")}
+    kw.setdefault("mu", 0.0)
     return do.Scheme(volume_flux=volume_flux, surface_flux=surface_flux, **kw)
 
 
@@ -33,6 +34,8 @@ def make_device(case: dict, volume_flux="chandrashekar", surface_flux="llf"):
     nd = case["ndims"]
     mesh = D.StructuredMesh(case["left"], case["right"], case["cells"])
     eq = D.CompressibleEuler2D(1.4) if nd == 2 else D.CompressibleEuler3D(1.4)
+    if case.get("viscous"):
+        eq = D.CompressibleNavierStokes2D(1.4, case["mu"], case["prandtl"])
     vflux = getattr(D, VF[volume_flux])
     if case.get("shock_capturing"):
         vi = D.VolumeIntegralShockCapturingHG(vflux)
@@ -51,7 +54,10 @@ def make_device(case: dict, volume_flux="chandrashekar", surface_flux="llf"):
 
 def initial(case: dict, s: do.Scheme, seed: int = 0):
     u = do.initial_state(s, case["ic"])
-    if case.get("noise"):
+    if case.get("viscous") and case.get("noise"):
+        rng = np.random.default_rng(seed)
+        u[..., 1:3] += case["noise"] * rng.standard_normal(u[..., 1:3].shape)
+    elif case.get("noise"):
         rng = np.random.default_rng(seed)
         u = u * (1.0 + case["noise"] * rng.standard_normal(u.shape))
     return u
@@ -86,7 +92,8 @@ def test_rhs_matches_reference(name, cuda):
     s = make_oracle(case)
     u = initial(case, s)
     kind = REF_KIND[(case["ic"], bool(case.get("shock_capturing")))]
-    rc = rb.RefCase(kind, case["polydeg"], case["cells"], case["left"], case["right"])
+    rc = rb.RefCase(kind, case["polydeg"], case["cells"], case["left"], case["right"],
+                    mu=case.get("mu", 0.0), prandtl=case.get("prandtl", 0.72))
     du_r = rc.rhs(u, 0.013)
     solver = make_device(case)
     du_d = device_rhs(solver, u, 0.013, cuda)
@@ -110,7 +117,7 @@ def test_indicator_flags_identical(name, cuda):
     assert flags.any()
 
 
-@pytest.mark.parametrize("name", ["kh", "dmr", "tgv"])
+@pytest.mark.parametrize("name", ["kh", "dmr", "tgv", "ns"])
 def test_ssprk3_step_matches_oracle(name, cuda):
     import torch
 
@@ -154,7 +161,7 @@ def test_other_fluxes_3d(vf, cuda):
     assert rel_linf(du_d, du_o) <= RTOL, rel_linf(du_d, du_o)
 
 
-@pytest.mark.parametrize("name", ["kh", "dmr", "tgv", "vortex_n6"])
+@pytest.mark.parametrize("name", ["kh", "dmr", "tgv", "vortex_n6", "ns"])
 def test_initial_condition_matches_oracle(name, cuda):
     import torch
 
@@ -165,7 +172,8 @@ def test_initial_condition_matches_oracle(name, cuda):
     solver = make_device(case)
     sol = D.Solution(solver.mesh, solver.basis, solver.eq)
     ic = {"kh": D.KelvinHelmholtzInitial(), "dmr": D.DoubleMachReflectionInitial(),
-          "tgv3d": D.InviscidTaylorGreenVortex(), "vortex": D.IsentropicVortex()}[case["ic"]]
+          "tgv3d": D.InviscidTaylorGreenVortex(), "vortex": D.IsentropicVortex(),
+          "tgv2d": D.TaylorGreenVortex2D()}[case["ic"]]
     solver.initialize(ic, sol)
     torch.cuda.synchronize()
     u_d = dev_to_ref(sol.u.cpu().numpy(), solver.mesh.n_cells)
@@ -183,3 +191,100 @@ def test_layout_round_trip(cuda):
     assert np.array_equal(back, u_ref)
     again = solver.from_reference_layout(torch.from_numpy(u_ref).to(cuda))
     assert torch.equal(again, ud)
+
+
+def test_graph_replay_equals_stream_steps(cuda):
+    """A captured CUDA graph of SSPRK3 steps (device clock for the
+    time-dependent DMR boundary state) reproduces stream launches bitwise."""
+    import ctypes
+
+    import torch
+
+    from dgsem_b200 import _capi as C
+    case = CASES["dmr"]
+    s = make_oracle(case)
+    u0 = torch.from_numpy(ref_to_dev(initial(case, s), 2)).to(cuda)
+    solver = make_device(case)
+    L, h = C.lib(), solver.handle
+    dt, t0 = 1.0e-4, 0.01
+    a = u0.clone()
+    C.check(L.dgsem_ssprk3_steps(h, ctypes.c_void_p(a.data_ptr()), t0, dt, 2), "steps")
+    b = u0.clone()
+    g = ctypes.c_void_p()
+    C.check(L.dgsem_graph_create(h, ctypes.c_void_p(b.data_ptr()), dt, 2, ctypes.byref(g)),
+            "graph")
+    C.check(L.dgsem_graph_launch(g, t0), "launch")
+    torch.cuda.synchronize()
+    C.check(L.dgsem_graph_destroy(g), "destroy")
+    assert torch.equal(a, b)
+
+
+def test_host_buffer_steps_equal_device_steps(cuda):
+    import ctypes
+
+    import torch
+
+    from dgsem_b200 import _capi as C
+    case = CASES["tgv"]
+    s = make_oracle(case)
+    u0 = torch.from_numpy(ref_to_dev(initial(case, s), 3)).to(cuda)
+    solver = make_device(case)
+    L, h = C.lib(), solver.handle
+    a = u0.clone()
+    C.check(L.dgsem_ssprk3_steps(h, ctypes.c_void_p(a.data_ptr()), 0.0, 1e-3, 3), "steps")
+    host = u0.cpu().pin_memory()
+    C.check(L.dgsem_ssprk3_steps_host(h, ctypes.c_void_p(host.data_ptr()), 0.0, 1e-3, 3),
+            "host steps")
+    torch.cuda.synchronize()
+    assert torch.equal(a.cpu(), host)
+
+
+def test_deterministic_and_nonfinite_flag(cuda):
+    import torch
+    case = CASES["kh_hg"]
+    s = make_oracle(case)
+    u = torch.from_numpy(ref_to_dev(initial(case, s), 2)).to(cuda)
+    solver = make_device(case)
+    d1, d2 = torch.empty_like(u), torch.empty_like(u)
+    solver.rhs(u, d1, 0.0)
+    solver.rhs(u, d2, 0.0)
+    torch.cuda.synchronize()
+    assert torch.equal(d1, d2)
+    solver.check_finite()
+    bad = u.clone()
+    bad[3, 0, 5] = float("nan")
+    solver.rhs(bad, d1, 0.0)
+    import dgsem_b200
+    with pytest.raises(dgsem_b200.DgsemError):
+        solver.check_finite()
+    solver.check_finite()  # flag cleared
+
+
+def test_conservation_and_free_stream_large(cuda):
+    """Size-independent properties at a benchmark size (TGV 16^3):
+    discrete conservation sum_i w_i J du_i = 0 and free-stream preservation."""
+    import torch
+
+    import dgsem_b200 as D
+    mesh = D.StructuredMesh((0.0,) * 3, (2 * np.pi,) * 3, (16, 16, 16))
+    solver = D.StructuredSolver(D.CompressibleEuler3D(1.4), D.LobattoLegendreBasis(3),
+                                D.VolumeIntegralSplitForm(D.KennedyGruberFlux),
+                                D.LaxFriedrichsFlux(), mesh,
+                                D.BoundarySet(*[D.PeriodicBC() for _ in range(6)]))
+    sol = D.Solution(mesh, D.LobattoLegendreBasis(3), D.CompressibleEuler3D(1.4))
+    solver.initialize(D.InviscidTaylorGreenVortex(), sol)
+    solver.calc_rhs(sol, 0.0)
+    w = torch.tensor(do.Basis(3).weights, dtype=torch.float64, device=cuda)
+    W = (w[None, None, :] * w[None, :, None] * w[:, None, None]).reshape(-1)
+    jac = (2 * np.pi / 16 / 2) ** 3
+    tot = (sol.du * W[None, None, :]).sum(dim=(0, 2)) * jac
+    assert float(tot.abs().max()) <= 1e-10 * float(sol.du.abs().max()) * sol.du.shape[0]
+    fs = torch.empty_like(sol.u)
+    fs[:, 0], fs[:, 1], fs[:, 2], fs[:, 3] = 1.0, 0.3, -0.2, 0.1
+    fs[:, 4] = 71.4 / 0.4 + 0.5 * (0.09 + 0.04 + 0.01)
+    du = torch.empty_like(fs)
+    solver.rhs(fs, du, 0.0)
+    # the residual is the reference metric round-off (~1e-12 relative in 3D,
+    # curl-form metrics) times the flux scale |u| / h
+    h = 2 * np.pi / 16
+    assert float(du.abs().max()) <= 1e-10 * float(fs.abs().max()) / h
