@@ -32,7 +32,7 @@
 
 namespace dgsem {
 
-constexpr int ipow(int b, int e) { return e == 0 ? 1 : b * ipow(b, e - 1); }
+__host__ __device__ constexpr int ipow(int b, int e) { return e == 0 ? 1 : b * ipow(b, e - 1); }
 
 template <int N>
 struct BasisConst {
@@ -259,6 +259,20 @@ __device__ __forceinline__ constexpr int padn(int node) {
   return node + node / N;
 }
 
+// Per-node shared-memory slots: the velocity, the flux-specific scalars and
+// -1/J.  Chandrashekar needs (p, beta, kin), Ranocha (p), Kennedy-Gruber
+// (p, e); p is always present because the surface fluxes use it.
+template <int DIM, int VF>
+struct NodeSlots {
+  static constexpr int P = DIM;
+  static constexpr int BETA = DIM + 1;  // beta (Chandrashekar) or e (Kennedy-Gruber)
+  static constexpr int KIN = DIM + 2;   // Chandrashekar only
+  static constexpr int NQ_FLUX = VF == VF_CHANDRASHEKAR ? DIM + 3
+                                 : VF == VF_KENNEDY_GRUBER ? DIM + 2 : DIM + 1;
+  static constexpr int MIJ = NQ_FLUX;   // -1/J
+  static constexpr int NQ = NQ_FLUX + 1;
+};
+
 template <int DIM, int N, int VF, int SF, bool HG, int EPB, bool NS = false>
 struct StageShape {
   static constexpr int NV = DIM + 2;
@@ -267,20 +281,16 @@ struct StageShape {
   static constexpr int NF = ipow(N, DIM - 1);
   static constexpr int NFACE = 2 * DIM;
   static constexpr int NLINE = DIM * NF;
-  // per node: v[DIM], p, beta, kin, sound speed, -1/J
-  static constexpr int NQ = DIM + 5;
-  static constexpr int Q_P = DIM, Q_BETA = DIM + 1, Q_KIN = DIM + 2, Q_A = DIM + 3,
-                       Q_MIJ = DIM + 4;
+  static constexpr int NQ = NodeSlots<DIM, VF>::NQ;
   static constexpr int SM_U = EPB * NV * NDP;
   static constexpr int SM_P = EPB * NQ * NDP;
-  static constexpr int SM_F = EPB * NFACE * NV * NF;
   static constexpr int SM_V = EPB * DIM * NV * NDP;
   static constexpr int SM_A = EPB;
   static constexpr int SM_W = NS ? EPB * DIM * NV * NDP : 0;  // -F_v [el][dim][var][node]
   // per element int info: ijk[3], eidx_other[3], neighbour[6] (-1 = boundary)
   static constexpr int NI = 12;
   static constexpr size_t smem_bytes =
-      sizeof(double) * (SM_U + SM_P + SM_F + SM_V + SM_A + SM_W) + sizeof(int) * EPB * NI;
+      sizeof(double) * (SM_U + SM_P + SM_V + SM_A + SM_W) + sizeof(int) * EPB * NI;
 };
 
 // Navier-Stokes pieces used by the stage kernel (defined in br1_kernel.cuh).
@@ -290,19 +300,286 @@ __device__ __forceinline__ void ns_neg_viscous_flux(const double* q, const doubl
                                                     const double* gy, double mu,
                                                     double kappa, int dim, double* f);
 
+// Element index over the axes != c of the element whose coordinate along
+// `dir` is replaced by `pos` (the neighbour across a face of direction dir).
+template <int DIM>
+__device__ __forceinline__ int eidx_other_shift(const int* I, int c, int dir, int pos,
+                                                int c0, int c1) {
+  if (c == dir) return I[3 + c];
+  if (DIM == 2) return pos;
+  const int ax0 = (c == 0) ? 1 : 0;  // first axis != c
+  const int ax1 = (c == 2) ? 1 : 2;  // second axis != c
+  const int i0 = (ax0 == dir) ? pos : I[ax0];
+  const int i1 = (ax1 == dir) ? pos : I[ax1];
+  return i0 + (ax0 == 0 ? c0 : c1) * i1;
+}
+
+// Interface or boundary flux f* at face node `line` of the face (dir, side)
+// of element `el` (surface_flux.hpp:45-271, boundary_set.hpp:70-86).
+template <int DIM, int N, int VF, int SF, bool NS, int NDP>
+__device__ __forceinline__ void element_face_flux(
+    const StageArgs<N>& p, const double* us_el, const double* pr_el, const double* wv_el,
+    const int* I, int dir, int side, int line, double gamma, double t_stage, int c0, int c1,
+    int c2, double* f) {
+  constexpr int NV = DIM + 2, ND = ipow(N, DIM);
+  using Q = NodeSlots<DIM, VF>;
+  const int own_node = line_node<DIM, N>(dir, line, side ? N - 1 : 0);
+  const int opn = padn<N>(own_node);
+  FaceState<DIM> so;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) so.u[q] = us_el[q * NDP + opn];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) so.v[d] = pr_el[d * NDP + opn];
+  so.p = pr_el[Q::P * NDP + opn];
+  so.a = sqrt(gamma * so.p / so.u[0]);
+  const int face = 2 * dir + side;
+  const int en = I[6 + face];
+  if (en >= 0) {
+    const int nb_node = line_node<DIM, N>(dir, line, side ? 0 : N - 1);
+    double un[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) un[q] = __ldg(p.u_in + ((int64_t)en * NV + q) * ND + nb_node);
+    const FaceState<DIM> sn = prepare_face<DIM>(un, gamma);
+    // normal: Ja^dir of the element on the high side at its low-face node
+    const int r_node = line_node<DIM, N>(dir, line, 0);
+    const int cells[3] = {c0, c1, c2};
+    int npos = I[dir] + 1;
+    if (npos >= cells[dir]) npos = 0;
+    double nrm[DIM];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      const int eo = side ? eidx_other_shift<DIM>(I, c, dir, npos, c0, c1) : I[3 + c];
+      nrm[c] = ja_at(p.tab.ja[dir][c], eo, ND, r_node);
+    }
+    if (side) {
+      surface_flux<DIM, SF>(so, sn, nrm, gamma, f);
+    } else {
+      surface_flux<DIM, SF>(sn, so, nrm, gamma, f);
+    }
+    if constexpr (NS) {
+      // one-sided viscous interface flux: -F_v . n of the high-side (primary)
+      // element at its low-face node (parabolic_viscous.hpp:570-585), lifted
+      // with the same factors as the inviscid flux
+      double w[2][4];
+      if (side) {
+        double q[4], gx[4], gy[4];
+        ns_gradient_variables(un, gamma, q);
+        const double* G = p.grad + (int64_t)en * 4 * 2 * ND + nb_node;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          gx[v] = __ldg(G + (v * 2 + 0) * ND);
+          gy[v] = __ldg(G + (v * 2 + 1) * ND);
+        }
+        ns_neg_viscous_flux(q, gx, gy, p.mu, p.kappa, 0, w[0]);
+        ns_neg_viscous_flux(q, gx, gy, p.mu, p.kappa, 1, w[1]);
+      } else {
+#pragma unroll
+        for (int d = 0; d < 2; ++d)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) w[d][v] = wv_el[(d * NV + v) * NDP + opn];
+      }
+#pragma unroll
+      for (int v = 0; v < 4; ++v) f[v] += w[0][v] * nrm[0] + w[1][v] * nrm[1];
+    }
+    return;
+  }
+  // boundary face (boundary_helper.hpp:93-146): own metric at the boundary
+  // node; the inner state is the left state on high faces.
+  double nrm[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) nrm[c] = ja_at(p.tab.ja[dir][c], I[3 + c], ND, own_node);
+  double ub[NV];
+  const int kind = p.bc.kind[face];
+  if (DIM == 2) {
+    const double x = __ldg(p.tab.coord[0] + I[0] * N + (own_node % N));
+    const double y = __ldg(p.tab.coord[1] + I[1] * N + (own_node / N));
+    if (kind == BC_DIRICHLET_DMR) {
+      dmr_state(p.bc, x, y, t_stage, ub);
+    } else if (kind == BC_DIRICHLET_CONST) {
+#pragma unroll
+      for (int q = 0; q < NV; ++q) ub[q] = p.bc.state[q];
+    } else if (kind == BC_OUTFLOW) {
+      // outflow_boundary.hpp:79-104: average along the line normal to the face
+#pragma unroll
+      for (int q = 0; q < NV; ++q) {
+        double acc = 0.0;
+#pragma unroll
+        for (int m = 0; m < N; ++m) acc += us_el[q * NDP + padn<N>(line_node<DIM, N>(dir, line, m))];
+        ub[q] = acc / (double)N;
+      }
+    } else if (kind == BC_MIXED_DMR_WALL && x < 1.0 / 6.0) {
+      dmr_state(p.bc, x, y, t_stage, ub);
+    } else {  // slip wall / wall branch of the mixed BC
+      reflect_state(so.u, nrm, ub);
+    }
+  }
+  const FaceState<DIM> sb = prepare_face<DIM>(ub, gamma);
+  if (side) {
+    surface_flux<DIM, SF>(so, sb, nrm, gamma, f);
+  } else {
+    surface_flux<DIM, SF>(sb, so, nrm, gamma, f);
+  }
+}
+
+// One line of direction DIR of element el: symmetric split-form pair loop
+// (each two-point flux evaluated once, both end nodes accumulated in
+// registers), viscous / FV terms, and the surface fluxes of the two faces the
+// line ends on, lifted into its end nodes.  DIR is a compile-time constant:
+// tasks are ordered direction-major so a warp never mixes directions.
+template <int DIR, int DIM, int N, int VF, int SF, bool HG, bool NS, int NDP, int NQ, int NI>
+__device__ __forceinline__ void process_line(const StageArgs<N>& p, const double* us,
+                                             const double* pr, double* dv,
+                                             const double* alpha_s, const double* wv,
+                                             const int* info, int el, int line, double gamma,
+                                             double t_stage, int c0, int c1, int c2) {
+  constexpr int NV = DIM + 2, ND = ipow(N, DIM);
+  using Q = NodeSlots<DIM, VF>;
+  constexpr int dir = DIR;
+  const int* I = info + el * NI;
+  const double* U = us + el * NV * NDP;
+  const double* P = pr + el * NQ * NDP;
+  double acc[N][NV];
+#pragma unroll
+  for (int m = 0; m < N; ++m)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) acc[m][q] = 0.0;
+  double ja[N][DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    const double* tab = p.tab.ja[dir][c] + (int64_t)I[3 + c] * ND;
+#pragma unroll
+    for (int m = 0; m < N; ++m) ja[m][c] = __ldg(tab + line_node<DIM, N>(dir, line, m));
+  }
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    const int ni = padn<N>(line_node<DIM, N>(dir, line, i));
+    NodeState<DIM> Li;
+    Li.rho = U[ni];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) Li.v[d] = P[d * NDP + ni];
+    Li.p = P[Q::P * NDP + ni];
+    Li.beta = VF == VF_RANOCHA ? 0.0 : P[Q::BETA * NDP + ni];
+    Li.kin = VF == VF_CHANDRASHEKAR ? P[Q::KIN * NDP + ni] : 0.0;
+#pragma unroll
+    for (int k = i + 1; k < N; ++k) {
+      const int nk = padn<N>(line_node<DIM, N>(dir, line, k));
+      NodeState<DIM> Rk;
+      Rk.rho = U[nk];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) Rk.v[d] = P[d * NDP + nk];
+      Rk.p = P[Q::P * NDP + nk];
+      Rk.beta = VF == VF_RANOCHA ? 0.0 : P[Q::BETA * NDP + nk];
+      Rk.kin = VF == VF_CHANDRASHEKAR ? P[Q::KIN * NDP + nk] : 0.0;
+      double nrm[DIM];
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) nrm[c] = 0.5 * (ja[i][c] + ja[k][c]);
+      double f[NV];
+      volume_flux<DIM, VF>(Li, Rk, nrm, p.inv_gm1, f);
+      const double dik = p.basis.Dsplit[i][k];
+      const double dki = p.basis.Dsplit[k][i];
+#pragma unroll
+      for (int q = 0; q < NV; ++q) {
+        acc[i][q] += dik * f[q];
+        acc[k][q] += dki * f[q];
+      }
+    }
+  }
+  if constexpr (NS) {
+    // viscous weak-form volume term along the line with Dhat on the
+    // contravariant flux Ja^dir . (-F_v) (parabolic_viscous.hpp:418-466)
+    double fc[N][NV];
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+      const int nm = padn<N>(line_node<DIM, N>(dir, line, m));
+#pragma unroll
+      for (int q = 0; q < NV; ++q)
+        fc[m][q] = ja[m][0] * wv[((el * 2 + 0) * NV + q) * NDP + nm] +
+                   ja[m][1] * wv[((el * 2 + 1) * NV + q) * NDP + nm];
+    }
+#pragma unroll
+    for (int m = 0; m < N; ++m)
+#pragma unroll
+      for (int k = 0; k < N; ++k)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) acc[m][q] += p.basis.Dhat[m][k] * fc[k][q];
+  }
+  if (HG) {
+    const double alpha = alpha_s[el];
+    if (fabs(alpha - 0.0) > p.atol) {
+      // volume_flux.hpp:830-841: (1 - alpha) * DG + alpha * FV
+      const double one_m = 1.0 - alpha;
+#pragma unroll
+      for (int m = 0; m < N; ++m)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) acc[m][q] *= one_m;
+      // volume_flux.hpp:457-509: LLF on subcell normals along the line
+      auto node_state = [&](int m) {
+        const int nm = padn<N>(line_node<DIM, N>(dir, line, m));
+        FaceState<DIM> st;
+#pragma unroll
+        for (int q = 0; q < NV; ++q) st.u[q] = U[q * NDP + nm];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) st.v[d] = P[d * NDP + nm];
+        st.p = P[Q::P * NDP + nm];
+        st.a = sqrt(gamma * st.p / st.u[0]);
+        return st;
+      };
+      FaceState<DIM> sl = node_state(0);
+#pragma unroll
+      for (int fi = 1; fi < N; ++fi) {
+        const FaceState<DIM> sr = node_state(fi);
+        double nrm[DIM];
+#pragma unroll
+        for (int c = 0; c < DIM; ++c)
+          nrm[c] = __ldg(p.tab.fv[dir][c] + (int64_t)I[3 + c] * (N - 1) * N + (fi - 1) * N + line);
+        double f[NV];
+        llf_flux<DIM>(sl, sr, nrm, f);
+        const double wl = alpha * p.basis.inv_w[fi - 1];
+        const double wr = alpha * p.basis.inv_w[fi];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+          acc[fi - 1][q] += wl * f[q];
+          acc[fi][q] -= wr * f[q];
+        }
+        sl = sr;
+      }
+    }
+  }
+  // surface fluxes at both ends of the line, lifted into the end nodes
+  // (surface_integral.hpp:35-154)
+  {
+    double f[NV];
+    element_face_flux<DIM, N, VF, SF, NS, NDP>(p, U, P, wv + el * 2 * NV * NDP, I, dir, 0,
+                                               line, gamma, t_stage, c0, c1, c2, f);
+#pragma unroll
+    for (int q = 0; q < NV; ++q) acc[0][q] -= f[q] * p.basis.lhat_l0;
+    element_face_flux<DIM, N, VF, SF, NS, NDP>(p, U, P, wv + el * 2 * NV * NDP, I, dir, 1,
+                                               line, gamma, t_stage, c0, c1, c2, f);
+#pragma unroll
+    for (int q = 0; q < NV; ++q) acc[N - 1][q] += f[q] * p.basis.lhat_rN;
+  }
+  double* V = dv + (el * DIM + dir) * NV * NDP;
+#pragma unroll
+  for (int m = 0; m < N; ++m) {
+    const int nm = padn<N>(line_node<DIM, N>(dir, line, m));
+#pragma unroll
+    for (int q = 0; q < NV; ++q) V[q * NDP + nm] = acc[m][q];
+  }
+}
+
 template <int DIM, int N, int VF, int SF, bool HG, int EPB, int NT, bool NS = false>
 __global__ void __launch_bounds__(NT)
     stage_kernel(const StageArgs<N> p) {
   using S = StageShape<DIM, N, VF, SF, HG, EPB, NS>;
+  using Q = NodeSlots<DIM, VF>;
   static_assert(!NS || (DIM == 2 && !HG), "Navier-Stokes: 2D split form only");
   static_assert(!HG || DIM == 2, "shock capturing: 2D only");
   constexpr int NV = S::NV, ND = S::ND, NDP = S::NDP, NF = S::NF, NFACE = S::NFACE,
                 NLINE = S::NLINE, NQ = S::NQ, NI = S::NI;
   extern __shared__ double smem[];
   double* us = smem;                 // [el][var][pnode]
-  double* pr = us + S::SM_U;         // [el][q][pnode]
-  double* fs = pr + S::SM_P;         // [el][face][var][fn]
-  double* dv = fs + S::SM_F;         // [el][dir][var][pnode]
+  double* pr = us + S::SM_U;         // [el][slot][pnode]
+  double* dv = pr + S::SM_P;         // [el][dir][var][pnode]
   double* alpha_s = dv + S::SM_V;    // [el]
   double* wv = alpha_s + S::SM_A;    // [el][dim][var][pnode] (NS)
   int* info = reinterpret_cast<int*>(wv + S::SM_W);
@@ -363,7 +640,7 @@ __global__ void __launch_bounds__(NT)
   }
   __syncthreads();
 
-  // ---- phase 1: node primitives, sound speed, -1/J, HG alpha --------------
+  // ---- phase 1: node primitives, -1/J, HG alpha, -F_v -----------------
   for (int idx = tid; idx < ne * ND; idx += NT) {
     const int el = idx / ND, node = idx % ND;
     const int pn = padn<N>(node);
@@ -374,10 +651,9 @@ __global__ void __launch_bounds__(NT)
     double* P = pr + el * NQ * NDP + pn;
 #pragma unroll
     for (int d = 0; d < DIM; ++d) P[d * NDP] = s.v[d];
-    P[S::Q_P * NDP] = s.p;
-    P[S::Q_BETA * NDP] = s.beta;
-    P[S::Q_KIN * NDP] = s.kin;
-    P[S::Q_A * NDP] = sqrt(gamma * s.p / u[0]);
+    P[Q::P * NDP] = s.p;
+    if (VF != VF_RANOCHA) P[Q::BETA * NDP] = s.beta;
+    if (VF == VF_CHANDRASHEKAR) P[Q::KIN * NDP] = s.kin;
     const int* I = info + el * NI;
     const int in = node % N, jn = (node / N) % N, kn = DIM == 3 ? node / (N * N) : 0;
     double jdet = __ldg(p.tab.jdiag[0] + I[0] * N + in);
@@ -386,7 +662,7 @@ __global__ void __launch_bounds__(NT)
     } else {
       jdet = jdet * (__ldg(p.tab.jdiag[1] + I[1] * N + jn) * __ldg(p.tab.jdiag[2] + I[2] * N + kn));
     }
-    P[S::Q_MIJ * NDP] = -(1.0 / jdet);
+    P[Q::MIJ * NDP] = -(1.0 / jdet);
     if constexpr (NS) {
       // -F_v at the node from the lifted gradient (parabolic_viscous.hpp:358-396)
       double q[4], gx[4], gy[4];
@@ -409,302 +685,51 @@ __global__ void __launch_bounds__(NT)
   if (HG) {
     for (int el = tid; el < ne; el += NT) {
       const double a = hg_alpha_2d<N, true>(us + el * NV * NDP, NDP, p.basis, p.hg_threshold,
-                                             p.hg_s, p.alpha_min, p.alpha_max);
+                                            p.hg_s, p.alpha_min, p.alpha_max);
       alpha_s[el] = a;
       if (p.alpha_out) p.alpha_out[e0 + el] = a;
     }
   }
   __syncthreads();
 
-  // ---- phase 2a: face fluxes ----------------------------------------------
-  for (int idx = tid; idx < ne * NFACE * NF; idx += NT) {
-    const int el = idx / (NFACE * NF);
-    const int face = (idx / NF) % NFACE;
-    const int fn = idx % NF;
-    const int dir = face >> 1, side = face & 1;
-    const int* I = info + el * NI;
-    const int own_node = face_node<DIM, N>(dir, fn, side ? N - 1 : 0);
-    const int opn = padn<N>(own_node);
-    FaceState<DIM> so;
-    {
-      const double* P = pr + el * NQ * NDP + opn;
-#pragma unroll
-      for (int q = 0; q < NV; ++q) so.u[q] = us[(el * NV + q) * NDP + opn];
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) so.v[d] = P[d * NDP];
-      so.p = P[S::Q_P * NDP];
-      so.a = P[S::Q_A * NDP];
-    }
-    const int en = I[6 + face];
-    double f[NV];
-    if (en >= 0) {
-      const int nb_node = face_node<DIM, N>(dir, fn, side ? 0 : N - 1);
-      double un[NV];
-#pragma unroll
-      for (int q = 0; q < NV; ++q)
-        un[q] = __ldg(p.u_in + ((int64_t)en * NV + q) * ND + nb_node);
-      const FaceState<DIM> sn = prepare_face<DIM>(un, gamma);
-      // normal: Ja^dir of the element on the high side at its low-face node
-      const int r_node = face_node<DIM, N>(dir, fn, 0);
-      double nrm[DIM];
-#pragma unroll
-      for (int c = 0; c < DIM; ++c) {
-        int eo;
-        if (side) {
-          // element-index over the axes != c of the neighbour: equal to ours
-          // unless c is the direction of the face
-          if (c == dir) {
-            eo = I[3 + c];
-          } else {
-            const int nq = (dir == 0) ? (en % c0)
-                         : (dir == 1) ? (DIM == 2 ? en / c0 : (en / c0) % c1)
-                                      : en / (c0 * c1);
-            if (DIM == 2) {
-              eo = nq;
-            } else {
-              const int ax0 = (c == 0) ? 1 : 0;         // first axis != c
-              const int ax1 = (c == 2) ? 1 : 2;         // second axis != c
-              const int i0 = (ax0 == dir) ? nq : I[ax0];
-              const int i1 = (ax1 == dir) ? nq : I[ax1];
-              eo = i0 + (ax0 == 0 ? c0 : c1) * i1;
-            }
-          }
-        } else {
-          eo = I[3 + c];
-        }
-        nrm[c] = ja_at(p.tab.ja[dir][c], eo, ND, r_node);
-      }
-      if (side) {
-        surface_flux<DIM, SF>(so, sn, nrm, gamma, f);
-      } else {
-        surface_flux<DIM, SF>(sn, so, nrm, gamma, f);
-      }
-      if constexpr (NS) {
-        // one-sided viscous interface flux: -F_v . n of the high-side
-        // (primary) element at its low-face node (parabolic_viscous.hpp:570-585);
-        // lifted with the same factors as the inviscid flux, so it is summed in.
-        double w[2][4];
-        if (side) {
-          double q[4], gx[4], gy[4];
-          ns_gradient_variables(un, gamma, q);
-          const double* G = p.grad + (int64_t)en * 4 * 2 * ND + nb_node;
-#pragma unroll
-          for (int v = 0; v < 4; ++v) {
-            gx[v] = __ldg(G + (v * 2 + 0) * ND);
-            gy[v] = __ldg(G + (v * 2 + 1) * ND);
-          }
-          ns_neg_viscous_flux(q, gx, gy, p.mu, p.kappa, 0, w[0]);
-          ns_neg_viscous_flux(q, gx, gy, p.mu, p.kappa, 1, w[1]);
-        } else {
-#pragma unroll
-          for (int d = 0; d < 2; ++d)
-#pragma unroll
-            for (int v = 0; v < 4; ++v) w[d][v] = wv[((el * 2 + d) * NV + v) * NDP + opn];
-        }
-#pragma unroll
-        for (int v = 0; v < 4; ++v) f[v] += w[0][v] * nrm[0] + w[1][v] * nrm[1];
-      }
-    } else {
-      // boundary_helper.hpp:93-146: own metric at the boundary node;
-      // inner state is the left state on high faces.
-      double nrm[DIM];
-#pragma unroll
-      for (int c = 0; c < DIM; ++c) nrm[c] = ja_at(p.tab.ja[dir][c], I[3 + c], ND, own_node);
-      double ub[NV];
-      const int kind = p.bc.kind[face];
-      if (DIM == 2) {
-        const double x = __ldg(p.tab.coord[0] + I[0] * N + (own_node % N));
-        const double y = __ldg(p.tab.coord[1] + I[1] * N + (own_node / N));
-        if (kind == BC_DIRICHLET_DMR) {
-          dmr_state(p.bc, x, y, t_stage, ub);
-        } else if (kind == BC_DIRICHLET_CONST) {
-#pragma unroll
-          for (int q = 0; q < NV; ++q) ub[q] = p.bc.state[q];
-        } else if (kind == BC_OUTFLOW) {
-          // outflow_boundary.hpp:79-104: average along the line normal to the face
-#pragma unroll
-          for (int q = 0; q < NV; ++q) {
-            double acc = 0.0;
-#pragma unroll
-            for (int m = 0; m < N; ++m)
-              acc += us[(el * NV + q) * NDP + padn<N>(face_node<DIM, N>(dir, fn, m))];
-            ub[q] = acc / (double)N;
-          }
-        } else if (kind == BC_MIXED_DMR_WALL && x < 1.0 / 6.0) {
-          dmr_state(p.bc, x, y, t_stage, ub);
-        } else {  // slip wall / wall branch of the mixed BC
-          reflect_state(so.u, nrm, ub);
-        }
-      }
-      const FaceState<DIM> sb = prepare_face<DIM>(ub, gamma);
-      if (side) {
-        surface_flux<DIM, SF>(so, sb, nrm, gamma, f);
-      } else {
-        surface_flux<DIM, SF>(sb, so, nrm, gamma, f);
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < NV; ++q) fs[((el * NFACE + face) * NV + q) * NF + fn] = f[q];
-  }
-
-  // ---- phase 2b: volume integral, one line per thread --------------------
+  // ---- phase 2: one line per thread: end-face fluxes + volume integral ------
   for (int idx = tid; idx < ne * NLINE; idx += NT) {
-    const int el = idx / NLINE;
-    const int dir = (idx % NLINE) / NF;
+    const int dir = idx / (ne * NF);
+    const int el = (idx / NF) % ne;
     const int line = idx % NF;
-    const int* I = info + el * NI;
-    const double* U = us + el * NV * NDP;
-    const double* P = pr + el * NQ * NDP;
-    double ja[N][DIM];
-#pragma unroll
-    for (int c = 0; c < DIM; ++c) {
-      const double* tab = p.tab.ja[dir][c] + (int64_t)I[3 + c] * ND;
-#pragma unroll
-      for (int m = 0; m < N; ++m) ja[m][c] = __ldg(tab + line_node<DIM, N>(dir, line, m));
-    }
-    double acc[N][NV];
-#pragma unroll
-    for (int m = 0; m < N; ++m)
-#pragma unroll
-      for (int q = 0; q < NV; ++q) acc[m][q] = 0.0;
-#pragma unroll
-    for (int i = 0; i < N; ++i) {
-      const int ni = padn<N>(line_node<DIM, N>(dir, line, i));
-      NodeState<DIM> Li;
-      Li.rho = U[ni];
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) Li.v[d] = P[d * NDP + ni];
-      Li.p = P[S::Q_P * NDP + ni];
-      Li.beta = P[S::Q_BETA * NDP + ni];
-      Li.kin = P[S::Q_KIN * NDP + ni];
-#pragma unroll
-      for (int k = i + 1; k < N; ++k) {
-        const int nk = padn<N>(line_node<DIM, N>(dir, line, k));
-        NodeState<DIM> Rk;
-        Rk.rho = U[nk];
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) Rk.v[d] = P[d * NDP + nk];
-        Rk.p = P[S::Q_P * NDP + nk];
-        Rk.beta = P[S::Q_BETA * NDP + nk];
-        Rk.kin = P[S::Q_KIN * NDP + nk];
-        double nrm[DIM];
-#pragma unroll
-        for (int c = 0; c < DIM; ++c) nrm[c] = 0.5 * (ja[i][c] + ja[k][c]);
-        double f[NV];
-        volume_flux<DIM, VF>(Li, Rk, nrm, p.inv_gm1, f);
-        const double dik = p.basis.Dsplit[i][k];
-        const double dki = p.basis.Dsplit[k][i];
-#pragma unroll
-        for (int q = 0; q < NV; ++q) {
-          acc[i][q] += dik * f[q];
-          acc[k][q] += dki * f[q];
-        }
-      }
-    }
-    if constexpr (NS) {
-      // viscous weak-form volume term along the line with Dhat on the
-      // contravariant flux Ja^dir . (-F_v) (parabolic_viscous.hpp:418-466)
-      double fc[N][NV];
-#pragma unroll
-      for (int m = 0; m < N; ++m) {
-        const int nm = padn<N>(line_node<DIM, N>(dir, line, m));
-#pragma unroll
-        for (int q = 0; q < NV; ++q)
-          fc[m][q] = ja[m][0] * wv[((el * 2 + 0) * NV + q) * NDP + nm] +
-                     ja[m][1] * wv[((el * 2 + 1) * NV + q) * NDP + nm];
-      }
-#pragma unroll
-      for (int m = 0; m < N; ++m)
-#pragma unroll
-        for (int k = 0; k < N; ++k)
-#pragma unroll
-          for (int q = 0; q < NV; ++q) acc[m][q] += p.basis.Dhat[m][k] * fc[k][q];
-    }
-    if (HG) {
-      const double alpha = alpha_s[el];
-      if (fabs(alpha - 0.0) > p.atol) {
-        // volume_flux.hpp:830-841: (1 - alpha) * DG + alpha * FV
-        const double one_m = 1.0 - alpha;
-#pragma unroll
-        for (int m = 0; m < N; ++m)
-#pragma unroll
-          for (int q = 0; q < NV; ++q) acc[m][q] *= one_m;
-        // volume_flux.hpp:457-509: LLF on subcell normals along the line
-        auto node_state = [&](int m) {
-          const int nm = padn<N>(line_node<DIM, N>(dir, line, m));
-          FaceState<DIM> st;
-#pragma unroll
-          for (int q = 0; q < NV; ++q) st.u[q] = U[q * NDP + nm];
-#pragma unroll
-          for (int d = 0; d < DIM; ++d) st.v[d] = P[d * NDP + nm];
-          st.p = P[S::Q_P * NDP + nm];
-          st.a = P[S::Q_A * NDP + nm];
-          return st;
-        };
-        FaceState<DIM> sl = node_state(0);
-#pragma unroll
-        for (int fi = 1; fi < N; ++fi) {
-          const FaceState<DIM> sr = node_state(fi);
-          double nrm[DIM];
-#pragma unroll
-          for (int c = 0; c < DIM; ++c)
-            nrm[c] = __ldg(p.tab.fv[dir][c] + (int64_t)I[3 + c] * (N - 1) * N + (fi - 1) * N + line);
-          double f[NV];
-          llf_flux<DIM>(sl, sr, nrm, f);
-          const double wl = alpha * p.basis.inv_w[fi - 1];
-          const double wr = alpha * p.basis.inv_w[fi];
-#pragma unroll
-          for (int q = 0; q < NV; ++q) {
-            acc[fi - 1][q] += wl * f[q];
-            acc[fi][q] -= wr * f[q];
-          }
-          sl = sr;
-        }
-      }
-    }
-    double* V = dv + (el * DIM + dir) * NV * NDP;
-#pragma unroll
-    for (int m = 0; m < N; ++m) {
-      const int nm = padn<N>(line_node<DIM, N>(dir, line, m));
-#pragma unroll
-      for (int q = 0; q < NV; ++q) V[q * NDP + nm] = acc[m][q];
+    if (dir == 0) {
+      process_line<0, DIM, N, VF, SF, HG, NS, NDP, NQ, NI>(p, us, pr, dv, alpha_s, wv, info, el,
+                                                          line, gamma, t_stage, c0, c1, c2);
+    } else if (DIM >= 2 && dir == 1) {
+      process_line<1, DIM, N, VF, SF, HG, NS, NDP, NQ, NI>(p, us, pr, dv, alpha_s, wv, info, el,
+                                                          line, gamma, t_stage, c0, c1, c2);
+    } else if (DIM == 3) {
+      process_line<(DIM == 3 ? 2 : 1), DIM, N, VF, SF, HG, NS, NDP, NQ, NI>(
+          p, us, pr, dv, alpha_s, wv, info, el, line, gamma, t_stage, c0, c1, c2);
     }
   }
   __syncthreads();
 
-  // ---- phase 3: lift, -1/J, SSPRK3 combination, store ---------------------
+  // ---- phase 3: sum of directions, -1/J, SSPRK3 combination, store -------
   bool bad = false;
   const int64_t gbase = (int64_t)e0 * NV * ND;
-  for (int idx = tid; idx < ne * NV * ND; idx += NT) {
-    const int el = idx / (NV * ND);
-    const int q = (idx / ND) % NV;
-    const int node = idx % ND;
+  for (int idx = tid; idx < ne * ND; idx += NT) {
+    const int el = idx / ND, node = idx % ND;
     const int pn = padn<N>(node);
-    double du = 0.0;
+    const double mij = pr[(el * NQ + Q::MIJ) * NDP + pn];
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) du += dv[((el * DIM + d) * NV + q) * NDP + pn];
-    const int in = node % N;
-    const int jn = (node / N) % N;
-    const int kn = (DIM == 3) ? node / (N * N) : 0;
-    const int pos[3] = {in, jn, kn};
+    for (int q = 0; q < NV; ++q) {
+      double du = 0.0;
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-      // face node index of this node on the faces normal to d
-      int fn;
-      if (DIM == 2) {
-        fn = (d == 0) ? jn : in;
-      } else {
-        fn = (d == 0) ? (jn + N * kn) : ((d == 1) ? (in + N * kn) : (in + N * jn));
-      }
-      if (pos[d] == 0) du -= fs[((el * NFACE + 2 * d) * NV + q) * NF + fn] * p.basis.lhat_l0;
-      if (pos[d] == N - 1) du += fs[((el * NFACE + 2 * d + 1) * NV + q) * NF + fn] * p.basis.lhat_rN;
+      for (int d = 0; d < DIM; ++d) du += dv[((el * DIM + d) * NV + q) * NDP + pn];
+      du = du * mij;
+      const int64_t gi = gbase + (int64_t)(el * NV + q) * ND + node;
+      double val = p.c * du;
+      if (p.b != 0.0) val = p.b * us[(el * NV + q) * NDP + pn] + val;
+      if (p.a != 0.0) val = p.a * p.u_n[gi] + val;
+      bad |= !isfinite(val);
+      p.out[gi] = val;
     }
-    du = du * pr[(el * NQ + S::Q_MIJ) * NDP + pn];
-    double val = p.c * du;
-    if (p.b != 0.0) val = p.b * us[(el * NV + q) * NDP + pn] + val;
-    if (p.a != 0.0) val = p.a * p.u_n[gbase + idx] + val;
-    bad |= !isfinite(val);
-    p.out[gbase + idx] = val;
   }
   if (bad) atomicOr(p.nonfinite, 1u);
 }
