@@ -184,9 +184,58 @@ __device__ __forceinline__ void reflect_state(const double* ui, const double* n,
 // Evaluated with explicitly rounded products and sums (no contraction) in
 // the reference's order, so alpha and the troubled-cell flag match.
 // ---------------------------------------------------------------------------
-// PAD selects the padded shared-memory node layout (node j*N+i stored at
-// j*(N+1)+i); ND is the stride between variables.
-template <int N, bool PAD = false>
+// Indicator variable rho * p with gamma fixed to 1.4 (indicator.hpp:148-161).
+__device__ __forceinline__ double hg_node_value(double rho, double m1, double m2,
+                                                double E) {
+  const double u_vel = __ddiv_rn(m1, rho);
+  const double v_vel = __ddiv_rn(m2, rho);
+  const double vv = __dadd_rn(__dmul_rn(u_vel, u_vel), __dmul_rn(v_vel, v_vel));
+  const double p = __dmul_rn(1.4 - 1.0, __dsub_rn(E, __dmul_rn(__dmul_rn(0.5, rho), vv)));
+  return __dmul_rn(p, rho);
+}
+
+// Modal energies -> logistic alpha with clipping (indicator.hpp:385-416).
+__device__ __forceinline__ double hg_alpha_from_energies(double total, double c1, double c2,
+                                                         double threshold, double s,
+                                                         double alpha_min,
+                                                         double alpha_max) {
+  const double e1 = (total != 0.0) ? __ddiv_rn(__dsub_rn(total, c1), total) : 0.0;
+  const double e2 = (c1 != 0.0) ? __ddiv_rn(__dsub_rn(c1, c2), c1) : 0.0;
+  const double energy = fmax(e1, e2);
+  double alpha = __ddiv_rn(
+      1.0, __dadd_rn(1.0, exp(__dmul_rn(__ddiv_rn(-s, threshold),
+                                        __dsub_rn(energy, threshold)))));
+  if (alpha < alpha_min) alpha = 0.0;
+  if (alpha > 1.0 - alpha_min) alpha = 1.0;
+  return fmin(alpha_max, alpha);
+}
+
+// Sequential energy sums over m2[j*N + i] in the reference's order
+// (total over all modes, clip1 over j,i < N-1, clip2 over j,i < N-2).
+template <int N>
+__device__ __forceinline__ void hg_energy_sums(const double* m2, double* total, double* c1,
+                                               double* c2) {
+  double t = 0.0, a = 0.0, b = 0.0;
+#pragma unroll
+  for (int j = 0; j < N; ++j)
+#pragma unroll
+    for (int i = 0; i < N; ++i) t = __dadd_rn(t, m2[j * N + i]);
+#pragma unroll
+  for (int j = 0; j + 1 < N; ++j)
+#pragma unroll
+    for (int i = 0; i + 1 < N; ++i) a = __dadd_rn(a, m2[j * N + i]);
+#pragma unroll
+  for (int j = 0; j + 2 < N; ++j)
+#pragma unroll
+    for (int i = 0; i + 2 < N; ++i) b = __dadd_rn(b, m2[j * N + i]);
+  *total = t;
+  *c1 = a;
+  *c2 = b;
+}
+
+// Single-thread version (standalone indicator kernel).  ND is the stride
+// between variables of the element's state.
+template <int N>
 __device__ double hg_alpha_2d(const double* us_el, int ND, const BasisConst<N>& B,
                               double threshold, double s, double alpha_min,
                               double alpha_max) {
@@ -195,14 +244,9 @@ __device__ double hg_alpha_2d(const double* us_el, int ND, const BasisConst<N>& 
   for (int j = 0; j < N; ++j)
 #pragma unroll
     for (int i = 0; i < N; ++i) {
-      const int node = PAD ? j * (N + 1) + i : j * N + i;
-      const double rho = us_el[0 * ND + node];
-      const double u_vel = __ddiv_rn(us_el[1 * ND + node], rho);
-      const double v_vel = __ddiv_rn(us_el[2 * ND + node], rho);
-      const double vv = __dadd_rn(__dmul_rn(u_vel, u_vel), __dmul_rn(v_vel, v_vel));
-      const double p = __dmul_rn(1.4 - 1.0, __dsub_rn(us_el[3 * ND + node],
-                                                       __dmul_rn(__dmul_rn(0.5, rho), vv)));
-      ind[j][i] = __dmul_rn(p, rho);
+      const int node = j * N + i;
+      ind[j][i] = hg_node_value(us_el[node], us_el[ND + node], us_el[2 * ND + node],
+                                us_el[3 * ND + node]);
     }
   double tmp[N][N];
 #pragma unroll
@@ -214,8 +258,7 @@ __device__ double hg_alpha_2d(const double* us_el, int ND, const BasisConst<N>& 
       for (int ii = 0; ii < N; ++ii) r = __dadd_rn(r, __dmul_rn(B.Vinv[i][ii], ind[j][ii]));
       tmp[j][i] = r;
     }
-  double total = 0.0, c1 = 0.0, c2 = 0.0;
-  double m2[N][N];
+  double m2[N * N];
 #pragma unroll
   for (int j = 0; j < N; ++j)
 #pragma unroll
@@ -223,29 +266,11 @@ __device__ double hg_alpha_2d(const double* us_el, int ND, const BasisConst<N>& 
       double r = 0.0;
 #pragma unroll
       for (int jj = 0; jj < N; ++jj) r = __dadd_rn(r, __dmul_rn(B.Vinv[j][jj], tmp[jj][i]));
-      m2[j][i] = __dmul_rn(r, r);
+      m2[j * N + i] = __dmul_rn(r, r);
     }
-#pragma unroll
-  for (int j = 0; j < N; ++j)
-#pragma unroll
-    for (int i = 0; i < N; ++i) total = __dadd_rn(total, m2[j][i]);
-#pragma unroll
-  for (int j = 0; j + 1 < N; ++j)
-#pragma unroll
-    for (int i = 0; i + 1 < N; ++i) c1 = __dadd_rn(c1, m2[j][i]);
-#pragma unroll
-  for (int j = 0; j + 2 < N; ++j)
-#pragma unroll
-    for (int i = 0; i + 2 < N; ++i) c2 = __dadd_rn(c2, m2[j][i]);
-  const double e1 = (total != 0.0) ? __ddiv_rn(__dsub_rn(total, c1), total) : 0.0;
-  const double e2 = (c1 != 0.0) ? __ddiv_rn(__dsub_rn(c1, c2), c1) : 0.0;
-  const double energy = fmax(e1, e2);
-  double alpha = __ddiv_rn(
-      1.0, __dadd_rn(1.0, exp(__dmul_rn(__ddiv_rn(-s, threshold),
-                                        __dsub_rn(energy, threshold)))));
-  if (alpha < alpha_min) alpha = 0.0;
-  if (alpha > 1.0 - alpha_min) alpha = 1.0;
-  return fmin(alpha_max, alpha);
+  double total, c1, c2;
+  hg_energy_sums<N>(m2, &total, &c1, &c2);
+  return hg_alpha_from_energies(total, c1, c2, threshold, s, alpha_min, alpha_max);
 }
 
 // ---------------------------------------------------------------------------
@@ -289,8 +314,9 @@ struct StageShape {
   static constexpr int SM_W = NS ? EPB * DIM * NV * NDP : 0;  // -F_v [el][dim][var][node]
   // per element int info: ijk[3], eidx_other[3], neighbour[6] (-1 = boundary)
   static constexpr int NI = 12;
+  static constexpr int SM_VINV = HG ? N * N : 0;
   static constexpr size_t smem_bytes =
-      sizeof(double) * (SM_U + SM_P + SM_V + SM_A + SM_W) + sizeof(int) * EPB * NI;
+      sizeof(double) * (SM_U + SM_P + SM_V + SM_A + SM_W + SM_VINV) + sizeof(int) * EPB * NI;
 };
 
 // Navier-Stokes pieces used by the stage kernel (defined in br1_kernel.cuh).
@@ -547,14 +573,31 @@ __device__ __forceinline__ void process_line(const StageArgs<N>& p, const double
   }
   // surface fluxes at both ends of the line, lifted into the end nodes
   // (surface_integral.hpp:35-154)
-  {
+  // Large face codes (HLLC, boundary states, viscous flux) are emitted once
+  // and called for both sides; small ones are specialised per side.
+  constexpr bool kCompactFaces = HG || SF == SF_HLLC || NS;
+  if constexpr (kCompactFaces) {
+#pragma unroll 1
+    for (int side = 0; side < 2; ++side) {
+      double f[NV];
+      element_face_flux<DIM, N, VF, SF, NS, NDP>(p, U, P, wv + el * 2 * NV * NDP, I, dir, side,
+                                                 line, gamma, t_stage, c0, c1, c2, f);
+      if (side == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) acc[0][q] -= f[q] * p.basis.lhat_l0;
+      } else {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) acc[N - 1][q] += f[q] * p.basis.lhat_rN;
+      }
+    }
+  } else {
     double f[NV];
-    element_face_flux<DIM, N, VF, SF, NS, NDP>(p, U, P, wv + el * 2 * NV * NDP, I, dir, 0,
-                                               line, gamma, t_stage, c0, c1, c2, f);
+    element_face_flux<DIM, N, VF, SF, NS, NDP>(p, U, P, wv + el * 2 * NV * NDP, I, dir, 0, line,
+                                               gamma, t_stage, c0, c1, c2, f);
 #pragma unroll
     for (int q = 0; q < NV; ++q) acc[0][q] -= f[q] * p.basis.lhat_l0;
-    element_face_flux<DIM, N, VF, SF, NS, NDP>(p, U, P, wv + el * 2 * NV * NDP, I, dir, 1,
-                                               line, gamma, t_stage, c0, c1, c2, f);
+    element_face_flux<DIM, N, VF, SF, NS, NDP>(p, U, P, wv + el * 2 * NV * NDP, I, dir, 1, line,
+                                               gamma, t_stage, c0, c1, c2, f);
 #pragma unroll
     for (int q = 0; q < NV; ++q) acc[N - 1][q] += f[q] * p.basis.lhat_rN;
   }
@@ -582,7 +625,8 @@ __global__ void __launch_bounds__(NT)
   double* dv = pr + S::SM_P;         // [el][dir][var][pnode]
   double* alpha_s = dv + S::SM_V;    // [el]
   double* wv = alpha_s + S::SM_A;    // [el][dim][var][pnode] (NS)
-  int* info = reinterpret_cast<int*>(wv + S::SM_W);
+  double* vinv_s = wv + S::SM_W;     // inverse Legendre Vandermonde (HG)
+  int* info = reinterpret_cast<int*>(vinv_s + S::SM_VINV);
 
   const int tid = threadIdx.x;
   const int e0 = (int)blockIdx.x * EPB;
@@ -630,6 +674,9 @@ __global__ void __launch_bounds__(NT)
       }
       I[6 + face] = nbr;
     }
+  }
+  if (HG) {
+    for (int k = tid; k < N * N; k += NT) vinv_s[k] = p.basis.Vinv[k / N][k % N];
   }
   {
     const double* src = p.u_in + (int64_t)e0 * NV * ND;
@@ -683,9 +730,43 @@ __global__ void __launch_bounds__(NT)
     }
   }
   if (HG) {
+    // Hennemann-Gassner alpha (indicator.hpp:337-418): node values, the two
+    // dimension-wise modal products, then the per-element sums; node-parallel
+    // with the scratch in the (not yet used) direction-contribution buffer.
+    __syncthreads();
+    double* ind = dv;                   // [el][ND]
+    double* tmp = dv + EPB * ND;        // [el][ND]
+    double* m2 = dv + 2 * EPB * ND;     // [el][ND]
+    for (int idx = tid; idx < ne * ND; idx += NT) {
+      const int el = idx / ND, node = idx % ND;
+      const int pn = padn<N>(node);
+      const double* Ue = us + el * NV * NDP;
+      ind[idx] = hg_node_value(Ue[pn], Ue[NDP + pn], Ue[2 * NDP + pn], Ue[3 * NDP + pn]);
+    }
+    __syncthreads();
+    for (int idx = tid; idx < ne * ND; idx += NT) {
+      const int el = idx / ND, node = idx % ND, j = node / N, i = node % N;
+      double r = 0.0;
+#pragma unroll
+      for (int ii = 0; ii < N; ++ii)
+        r = __dadd_rn(r, __dmul_rn(vinv_s[i * N + ii], ind[el * ND + j * N + ii]));
+      tmp[idx] = r;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < ne * ND; idx += NT) {
+      const int el = idx / ND, node = idx % ND, j = node / N, i = node % N;
+      double r = 0.0;
+#pragma unroll
+      for (int jj = 0; jj < N; ++jj)
+        r = __dadd_rn(r, __dmul_rn(vinv_s[j * N + jj], tmp[el * ND + jj * N + i]));
+      m2[idx] = __dmul_rn(r, r);
+    }
+    __syncthreads();
     for (int el = tid; el < ne; el += NT) {
-      const double a = hg_alpha_2d<N, true>(us + el * NV * NDP, NDP, p.basis, p.hg_threshold,
-                                            p.hg_s, p.alpha_min, p.alpha_max);
+      double total, c1, c2;
+      hg_energy_sums<N>(m2 + el * ND, &total, &c1, &c2);
+      const double a = hg_alpha_from_energies(total, c1, c2, p.hg_threshold, p.hg_s,
+                                              p.alpha_min, p.alpha_max);
       alpha_s[el] = a;
       if (p.alpha_out) p.alpha_out[e0 + el] = a;
     }
