@@ -35,6 +35,10 @@ EXPORTED = [
     "dgsem_from_reference_layout", "dgsem_check_finite", "dgsem_launch_count",
     "dgsem_basis_tables_host", "dgsem_metrics_host", "dgsem_ssprk3_steps_host",
     "dgsem_graph_create", "dgsem_graph_launch", "dgsem_graph_destroy",
+    "dgsem_batch_create", "dgsem_batch_destroy", "dgsem_batch_offsets",
+    "dgsem_batch_initial_condition", "dgsem_batch_ssprk3_step", "dgsem_batch_graph_create",
+    "dgsem_batch_graph_launch", "dgsem_batch_graph_destroy", "dgsem_batch_check_finite",
+    "dgsem_batch_launch_count",
 ]
 
 
@@ -98,6 +102,18 @@ def lib() -> ctypes.CDLL:
     L.dgsem_graph_create.argtypes = [vp, dp, c.c_double, c.c_int, c.POINTER(vp)]
     L.dgsem_graph_launch.argtypes = [vp, c.c_double]
     L.dgsem_graph_destroy.argtypes = [vp]
+    L.dgsem_batch_create.argtypes = [c.POINTER(MeshDesc), c.c_int, c.POINTER(SchemeDesc), vp,
+                                     c.POINTER(vp)]
+    L.dgsem_batch_destroy.argtypes = [vp]
+    L.dgsem_batch_offsets.argtypes = [vp, c.POINTER(c.c_int64)]
+    L.dgsem_batch_initial_condition.argtypes = [vp, c.c_int, c.POINTER(c.c_double), dp]
+    L.dgsem_batch_ssprk3_step.argtypes = [vp, dp, c.c_double, c.POINTER(c.c_double)]
+    L.dgsem_batch_graph_create.argtypes = [vp, dp, c.POINTER(c.c_double), c.c_int,
+                                           c.POINTER(vp)]
+    L.dgsem_batch_graph_launch.argtypes = [vp]
+    L.dgsem_batch_graph_destroy.argtypes = [vp]
+    L.dgsem_batch_check_finite.argtypes = [vp]
+    L.dgsem_batch_launch_count.argtypes = [vp, c.POINTER(c.c_int64)]
     for name in EXPORTED:
         f = getattr(L, name)
         if name != "dgsem_status_string":

@@ -576,22 +576,33 @@ dgsem_status dgsem_indicator(dgsem_ctx* ctx, const double* u, double* alpha,
   return cuda_status(cudaGetLastError());
 }
 
+}  // extern "C"
+
+namespace dgsem {
+cudaError_t launch_initial(int kind, int ndims, int n, const int64_t* cells, int64_t nelem,
+                           const DeviceTables& tab, const BcParams& bc, double gamma,
+                           const double* params, double* u, cudaStream_t s) {
+  const int nodes = ndims == 2 ? n * n : n * n * n;
+  const int64_t total = nelem * nodes;
+  const int threads = 256;
+  initial_kernel<<<(unsigned)((total + threads - 1) / threads), threads, 0, s>>>(
+      kind, ndims, n, cells[0], cells[1], nelem, tab, bc, gamma, params ? params[0] : 0.0,
+      params ? params[1] : 0.0, params ? params[2] : 0.0, params ? 1 : 0, u);
+  return cudaGetLastError();
+}
+}  // namespace dgsem
+
+extern "C" {
+
 dgsem_status dgsem_initial_condition(dgsem_ctx* ctx, int kind,
                                      const double* params, double* u) {
   if (!ctx || !u || kind < 0 || kind > 4) return DGSEM_ERR_INVALID_ARG;
   const EngineConfig& c = ctx->cfg;
   const bool want3 = kind == DGSEM_IC_TAYLOR_GREEN_3D;
   if (want3 != (c.ndims == 3)) return DGSEM_ERR_INVALID_ARG;
-  const int64_t total = c.nelem * ctx->nodes;
-  const int threads = 256;
-  initial_kernel<<<(unsigned)((total + threads - 1) / threads), threads, 0,
-                   ctx->stream>>>(kind, c.ndims, c.n, c.cells[0], c.cells[1],
-                                  c.nelem, c.tab, c.bc, c.gamma,
-                                  params ? params[0] : 0.0,
-                                  params ? params[1] : 0.0,
-                                  params ? params[2] : 0.0, params ? 1 : 0, u);
   ctx->launches++;
-  return cuda_status(cudaGetLastError());
+  return cuda_status(launch_initial(kind, c.ndims, c.n, c.cells, c.nelem, c.tab, c.bc, c.gamma,
+                                    params, u, ctx->stream));
 }
 
 static dgsem_status layout(dgsem_ctx* ctx, const double* src, double* dst,

@@ -40,6 +40,13 @@ class EngineBase {
                             const double* u_in, double* out, double a, double b,
                             double c, double t, const double* t_dev,
                             double* alpha_out, cudaStream_t s) = 0;
+  // Batched launch over a tile list (mesh index and first element per block)
+  // of meshes sharing this engine's scheme and degree; per-mesh data in
+  // `meshes` (device array).
+  virtual cudaError_t batch_stage(const EngineConfig& cfg, const MeshView* meshes,
+                                  const int* tile_mesh, const int* tile_e0, int ntiles,
+                                  double a, double b, double t, const double* t_dev,
+                                  cudaStream_t s) = 0;
   virtual int kernels_per_stage() const = 0;
   virtual int elements_per_block() const = 0;
   virtual int threads_per_block() const = 0;
@@ -48,6 +55,11 @@ class EngineBase {
 
 std::unique_ptr<EngineBase> make_engine(int ndims, int n, int vf, int sf,
                                         bool hg, bool ns);
+
+// Nodal initial condition on one mesh (capi.cu).
+cudaError_t launch_initial(int kind, int ndims, int n, const int64_t* cells, int64_t nelem,
+                           const DeviceTables& tab, const BcParams& bc, double gamma,
+                           const double* params, double* u, cudaStream_t s);
 
 template <int N>
 inline void fill_basis_const(const BasisTables& b, BasisConst<N>* out) {
@@ -85,26 +97,19 @@ class Engine final : public EngineBase {
     cudaFuncSetAttribute(stage_kernel<DIM, N, VF, SF, HG, EPB, NT, NS>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)Shape::smem_bytes);
+    if constexpr (!NS && !HG)
+      cudaFuncSetAttribute(stage_kernel<DIM, N, VF, SF, HG, EPB, NT, NS, true>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)Shape::smem_bytes);
   }
 
-  cudaError_t stage(const EngineConfig& cfg, const double* u_n,
-                    const double* u_in, double* out, double a, double b,
-                    double c, double t, const double* t_dev,
-                    double* alpha_out, cudaStream_t s) override {
-    StageArgs<N> args;
-    args.u_in = u_in;
-    args.u_n = u_n;
-    args.out = out;
+  StageArgs<N> common_args(const EngineConfig& cfg, double a, double b, double t,
+                           const double* t_dev, double* alpha_out) const {
+    StageArgs<N> args{};
     args.a = a;
     args.b = b;
-    args.c = c;
     args.t = t;
     args.t_dev = t_dev;
-    for (int i = 0; i < 3; ++i) {
-      args.cells[i] = cfg.cells[i];
-      args.periodic[i] = cfg.periodic[i];
-    }
-    args.nelem = cfg.nelem;
     args.gamma = cfg.gamma;
     args.inv_gm1 = 1.0 / (cfg.gamma - 1.0);
     args.alpha_max = cfg.alpha_max;
@@ -117,9 +122,26 @@ class Engine final : public EngineBase {
     args.grad = cfg.grad;
     args.mu = cfg.mu;
     args.kappa = cfg.gamma / ((cfg.gamma - 1.0) * cfg.prandtl);
-    args.tab = cfg.tab;
     args.bc = cfg.bc;
     fill_basis_const<N>(cfg.basis, &args.basis);
+    return args;
+  }
+
+  cudaError_t stage(const EngineConfig& cfg, const double* u_n,
+                    const double* u_in, double* out, double a, double b,
+                    double c, double t, const double* t_dev,
+                    double* alpha_out, cudaStream_t s) override {
+    StageArgs<N> args = common_args(cfg, a, b, t, t_dev, alpha_out);
+    args.mesh.u_in = u_in;
+    args.mesh.u_n = u_n;
+    args.mesh.out = out;
+    args.mesh.c = c;
+    for (int i = 0; i < 3; ++i) {
+      args.mesh.cells[i] = (int)cfg.cells[i];
+      args.mesh.periodic[i] = cfg.periodic[i];
+    }
+    args.mesh.nelem = (int)cfg.nelem;
+    args.mesh.tab = cfg.tab;
     if constexpr (NS) {
       GradArgs<N> ga;
       ga.u = u_in;
@@ -137,6 +159,23 @@ class Engine final : public EngineBase {
     stage_kernel<DIM, N, VF, SF, HG, EPB, NT, NS>
         <<<(unsigned)blocks, NT, Shape::smem_bytes, s>>>(args);
     return cudaGetLastError();
+  }
+
+  cudaError_t batch_stage(const EngineConfig& cfg, const MeshView* meshes,
+                          const int* tile_mesh, const int* tile_e0, int ntiles,
+                          double a, double b, double t, const double* t_dev,
+                          cudaStream_t s) override {
+    if constexpr (NS || HG) {
+      return cudaErrorNotSupported;
+    } else {
+      StageArgs<N> args = common_args(cfg, a, b, t, t_dev, nullptr);
+      args.meshes = meshes;
+      args.tile_mesh = tile_mesh;
+      args.tile_e0 = tile_e0;
+      stage_kernel<DIM, N, VF, SF, HG, EPB, NT, NS, true>
+          <<<(unsigned)ntiles, NT, Shape::smem_bytes, s>>>(args);
+      return cudaGetLastError();
+    }
   }
   int kernels_per_stage() const override { return NS ? 2 : 1; }
   int elements_per_block() const override { return EPB; }

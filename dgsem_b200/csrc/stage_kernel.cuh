@@ -68,25 +68,35 @@ struct BcParams {
   double sqrt3;
 };
 
-template <int N>
-struct StageArgs {
+// Per-mesh data of one stage launch.  A block stages its mesh's view into
+// shared memory at start: single-mesh launches copy it from the kernel
+// parameters, batched launches from the per-tile mesh list.
+struct MeshView {
   const double* u_in;
   const double* u_n;
   double* out;
-  double a, b, c;  // out = a*u_n + b*u_in + c*du
-  double t;             // stage time when t_dev is null
-  const double* t_dev;  // optional device clock: stage time = *t_dev + t
-
-  int64_t cells[3];
-  int64_t nelem;
+  double c;  // out = a*u_n + b*u_in + c*du  (c = stage factor * this mesh's dt)
+  int cells[3];
+  int nelem;
   int periodic[3];
+  DeviceTables tab;
+};
+
+template <int N>
+struct StageArgs {
+  MeshView mesh;           // single-mesh launches
+  const MeshView* meshes;  // batched launches: mesh table
+  const int* tile_mesh;    // batched launches: mesh of each block
+  const int* tile_e0;      // batched launches: first element of each block
+  double a, b;             // out = a*u_n + b*u_in + c*du
+  double t;                // stage time when t_dev is null
+  const double* t_dev;     // optional device clock: stage time = *t_dev + t
   double gamma, inv_gm1;
   double alpha_max, alpha_min, atol, hg_threshold, hg_s;
-  double* alpha_out;  // optional per-element alpha
+  double* alpha_out;       // optional per-element alpha
   unsigned int* nonfinite;
-  const double* grad;  // Navier-Stokes lifted gradient [E][4][2][ND]
+  const double* grad;      // Navier-Stokes lifted gradient [E][4][2][ND]
   double mu, kappa;
-  DeviceTables tab;
   BcParams bc;
   BasisConst<N> basis;
 };
@@ -344,7 +354,7 @@ __device__ __forceinline__ int eidx_other_shift(const int* I, int c, int dir, in
 // of element `el` (surface_flux.hpp:45-271, boundary_set.hpp:70-86).
 template <int DIM, int N, int VF, int SF, bool NS, int NDP>
 __device__ __forceinline__ void element_face_flux(
-    const StageArgs<N>& p, const double* us_el, const double* pr_el, const double* wv_el,
+    const StageArgs<N>& p, const MeshView& M, const double* us_el, const double* pr_el, const double* wv_el,
     const int* I, int dir, int side, int line, double gamma, double t_stage, int c0, int c1,
     int c2, double* f) {
   constexpr int NV = DIM + 2, ND = ipow(N, DIM);
@@ -364,7 +374,7 @@ __device__ __forceinline__ void element_face_flux(
     const int nb_node = line_node<DIM, N>(dir, line, side ? 0 : N - 1);
     double un[NV];
 #pragma unroll
-    for (int q = 0; q < NV; ++q) un[q] = __ldg(p.u_in + ((int64_t)en * NV + q) * ND + nb_node);
+    for (int q = 0; q < NV; ++q) un[q] = __ldg(M.u_in + ((int64_t)en * NV + q) * ND + nb_node);
     const FaceState<DIM> sn = prepare_face<DIM>(un, gamma);
     // normal: Ja^dir of the element on the high side at its low-face node
     const int r_node = line_node<DIM, N>(dir, line, 0);
@@ -375,7 +385,7 @@ __device__ __forceinline__ void element_face_flux(
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
       const int eo = side ? eidx_other_shift<DIM>(I, c, dir, npos, c0, c1) : I[3 + c];
-      nrm[c] = ja_at(p.tab.ja[dir][c], eo, ND, r_node);
+      nrm[c] = ja_at(M.tab.ja[dir][c], eo, ND, r_node);
     }
     if (side) {
       surface_flux<DIM, SF>(so, sn, nrm, gamma, f);
@@ -413,12 +423,12 @@ __device__ __forceinline__ void element_face_flux(
   // node; the inner state is the left state on high faces.
   double nrm[DIM];
 #pragma unroll
-  for (int c = 0; c < DIM; ++c) nrm[c] = ja_at(p.tab.ja[dir][c], I[3 + c], ND, own_node);
+  for (int c = 0; c < DIM; ++c) nrm[c] = ja_at(M.tab.ja[dir][c], I[3 + c], ND, own_node);
   double ub[NV];
   const int kind = p.bc.kind[face];
   if (DIM == 2) {
-    const double x = __ldg(p.tab.coord[0] + I[0] * N + (own_node % N));
-    const double y = __ldg(p.tab.coord[1] + I[1] * N + (own_node / N));
+    const double x = __ldg(M.tab.coord[0] + I[0] * N + (own_node % N));
+    const double y = __ldg(M.tab.coord[1] + I[1] * N + (own_node / N));
     if (kind == BC_DIRICHLET_DMR) {
       dmr_state(p.bc, x, y, t_stage, ub);
     } else if (kind == BC_DIRICHLET_CONST) {
@@ -453,7 +463,8 @@ __device__ __forceinline__ void element_face_flux(
 // line ends on, lifted into its end nodes.  DIR is a compile-time constant:
 // tasks are ordered direction-major so a warp never mixes directions.
 template <int DIR, int DIM, int N, int VF, int SF, bool HG, bool NS, int NDP, int NQ, int NI>
-__device__ __forceinline__ void process_line(const StageArgs<N>& p, const double* us,
+__device__ __forceinline__ void process_line(const StageArgs<N>& p, const MeshView& M,
+                                             const double* us,
                                              const double* pr, double* dv,
                                              const double* alpha_s, const double* wv,
                                              const int* info, int el, int line, double gamma,
@@ -472,7 +483,7 @@ __device__ __forceinline__ void process_line(const StageArgs<N>& p, const double
   double ja[N][DIM];
 #pragma unroll
   for (int c = 0; c < DIM; ++c) {
-    const double* tab = p.tab.ja[dir][c] + (int64_t)I[3 + c] * ND;
+    const double* tab = M.tab.ja[dir][c] + (int64_t)I[3 + c] * ND;
 #pragma unroll
     for (int m = 0; m < N; ++m) ja[m][c] = __ldg(tab + line_node<DIM, N>(dir, line, m));
   }
@@ -557,7 +568,7 @@ __device__ __forceinline__ void process_line(const StageArgs<N>& p, const double
         double nrm[DIM];
 #pragma unroll
         for (int c = 0; c < DIM; ++c)
-          nrm[c] = __ldg(p.tab.fv[dir][c] + (int64_t)I[3 + c] * (N - 1) * N + (fi - 1) * N + line);
+          nrm[c] = __ldg(M.tab.fv[dir][c] + (int64_t)I[3 + c] * (N - 1) * N + (fi - 1) * N + line);
         double f[NV];
         llf_flux<DIM>(sl, sr, nrm, f);
         const double wl = alpha * p.basis.inv_w[fi - 1];
@@ -580,7 +591,7 @@ __device__ __forceinline__ void process_line(const StageArgs<N>& p, const double
 #pragma unroll 1
     for (int side = 0; side < 2; ++side) {
       double f[NV];
-      element_face_flux<DIM, N, VF, SF, NS, NDP>(p, U, P, wv + el * 2 * NV * NDP, I, dir, side,
+      element_face_flux<DIM, N, VF, SF, NS, NDP>(p, M, U, P, wv + el * 2 * NV * NDP, I, dir, side,
                                                  line, gamma, t_stage, c0, c1, c2, f);
       if (side == 0) {
 #pragma unroll
@@ -592,11 +603,11 @@ __device__ __forceinline__ void process_line(const StageArgs<N>& p, const double
     }
   } else {
     double f[NV];
-    element_face_flux<DIM, N, VF, SF, NS, NDP>(p, U, P, wv + el * 2 * NV * NDP, I, dir, 0, line,
+    element_face_flux<DIM, N, VF, SF, NS, NDP>(p, M, U, P, wv + el * 2 * NV * NDP, I, dir, 0, line,
                                                gamma, t_stage, c0, c1, c2, f);
 #pragma unroll
     for (int q = 0; q < NV; ++q) acc[0][q] -= f[q] * p.basis.lhat_l0;
-    element_face_flux<DIM, N, VF, SF, NS, NDP>(p, U, P, wv + el * 2 * NV * NDP, I, dir, 1, line,
+    element_face_flux<DIM, N, VF, SF, NS, NDP>(p, M, U, P, wv + el * 2 * NV * NDP, I, dir, 1, line,
                                                gamma, t_stage, c0, c1, c2, f);
 #pragma unroll
     for (int q = 0; q < NV; ++q) acc[N - 1][q] += f[q] * p.basis.lhat_rN;
@@ -610,7 +621,8 @@ __device__ __forceinline__ void process_line(const StageArgs<N>& p, const double
   }
 }
 
-template <int DIM, int N, int VF, int SF, bool HG, int EPB, int NT, bool NS = false>
+template <int DIM, int N, int VF, int SF, bool HG, int EPB, int NT, bool NS = false,
+          bool BATCH = false>
 __global__ void __launch_bounds__(NT)
     stage_kernel(const StageArgs<N> p) {
   using S = StageShape<DIM, N, VF, SF, HG, EPB, NS>;
@@ -629,13 +641,23 @@ __global__ void __launch_bounds__(NT)
   int* info = reinterpret_cast<int*>(vinv_s + S::SM_VINV);
 
   const int tid = threadIdx.x;
-  const int e0 = (int)blockIdx.x * EPB;
-  const int nelem = (int)p.nelem;
+  __shared__ MeshView mesh_s;
+  int e0;
+  if constexpr (BATCH) {
+    e0 = p.tile_e0[blockIdx.x];
+    if (tid == 0) mesh_s = p.meshes[p.tile_mesh[blockIdx.x]];
+  } else {
+    e0 = (int)blockIdx.x * EPB;
+    if (tid == 0) mesh_s = p.mesh;
+  }
+  __syncthreads();
+  const MeshView& M = mesh_s;
+  const int nelem = M.nelem;
   if (e0 >= nelem) return;
   const int ne = min(EPB, nelem - e0);
   const double gamma = p.gamma;
   const double t_stage = p.t_dev ? (*p.t_dev + p.t) : p.t;
-  const int c0 = (int)p.cells[0], c1 = (int)p.cells[1], c2 = (int)p.cells[2];
+  const int c0 = M.cells[0], c1 = M.cells[1], c2 = M.cells[2];
 
   // ---- phase 0: element info and the contiguous u_in tile ----------------
   for (int el = tid; el < ne; el += NT) {
@@ -664,7 +686,7 @@ __global__ void __launch_bounds__(NT)
       int pos = ijk[dir] + (side ? 1 : -1);
       int nbr = -1;
       if (pos < 0 || pos >= cells[dir]) {
-        if (p.periodic[dir]) pos = (pos + cells[dir]) % cells[dir];
+        if (M.periodic[dir]) pos = (pos + cells[dir]) % cells[dir];
         else pos = -1;
       }
       if (pos >= 0) {
@@ -679,7 +701,7 @@ __global__ void __launch_bounds__(NT)
     for (int k = tid; k < N * N; k += NT) vinv_s[k] = p.basis.Vinv[k / N][k % N];
   }
   {
-    const double* src = p.u_in + (int64_t)e0 * NV * ND;
+    const double* src = M.u_in + (int64_t)e0 * NV * ND;
     for (int idx = tid; idx < ne * NV * ND; idx += NT) {
       const int row = idx / ND, node = idx % ND;
       us[row * NDP + padn<N>(node)] = __ldg(src + idx);
@@ -703,11 +725,11 @@ __global__ void __launch_bounds__(NT)
     if (VF == VF_CHANDRASHEKAR) P[Q::KIN * NDP] = s.kin;
     const int* I = info + el * NI;
     const int in = node % N, jn = (node / N) % N, kn = DIM == 3 ? node / (N * N) : 0;
-    double jdet = __ldg(p.tab.jdiag[0] + I[0] * N + in);
+    double jdet = __ldg(M.tab.jdiag[0] + I[0] * N + in);
     if (DIM == 2) {
-      jdet = jdet * __ldg(p.tab.jdiag[1] + I[1] * N + jn);
+      jdet = jdet * __ldg(M.tab.jdiag[1] + I[1] * N + jn);
     } else {
-      jdet = jdet * (__ldg(p.tab.jdiag[1] + I[1] * N + jn) * __ldg(p.tab.jdiag[2] + I[2] * N + kn));
+      jdet = jdet * (__ldg(M.tab.jdiag[1] + I[1] * N + jn) * __ldg(M.tab.jdiag[2] + I[2] * N + kn));
     }
     P[Q::MIJ * NDP] = -(1.0 / jdet);
     if constexpr (NS) {
@@ -779,14 +801,14 @@ __global__ void __launch_bounds__(NT)
     const int el = (idx / NF) % ne;
     const int line = idx % NF;
     if (dir == 0) {
-      process_line<0, DIM, N, VF, SF, HG, NS, NDP, NQ, NI>(p, us, pr, dv, alpha_s, wv, info, el,
+      process_line<0, DIM, N, VF, SF, HG, NS, NDP, NQ, NI>(p, M, us, pr, dv, alpha_s, wv, info, el,
                                                           line, gamma, t_stage, c0, c1, c2);
     } else if (DIM >= 2 && dir == 1) {
-      process_line<1, DIM, N, VF, SF, HG, NS, NDP, NQ, NI>(p, us, pr, dv, alpha_s, wv, info, el,
+      process_line<1, DIM, N, VF, SF, HG, NS, NDP, NQ, NI>(p, M, us, pr, dv, alpha_s, wv, info, el,
                                                           line, gamma, t_stage, c0, c1, c2);
     } else if (DIM == 3) {
       process_line<(DIM == 3 ? 2 : 1), DIM, N, VF, SF, HG, NS, NDP, NQ, NI>(
-          p, us, pr, dv, alpha_s, wv, info, el, line, gamma, t_stage, c0, c1, c2);
+          p, M, us, pr, dv, alpha_s, wv, info, el, line, gamma, t_stage, c0, c1, c2);
     }
   }
   __syncthreads();
@@ -805,11 +827,11 @@ __global__ void __launch_bounds__(NT)
       for (int d = 0; d < DIM; ++d) du += dv[((el * DIM + d) * NV + q) * NDP + pn];
       du = du * mij;
       const int64_t gi = gbase + (int64_t)(el * NV + q) * ND + node;
-      double val = p.c * du;
+      double val = M.c * du;
       if (p.b != 0.0) val = p.b * us[(el * NV + q) * NDP + pn] + val;
-      if (p.a != 0.0) val = p.a * p.u_n[gi] + val;
+      if (p.a != 0.0) val = p.a * M.u_n[gi] + val;
       bad |= !isfinite(val);
-      p.out[gi] = val;
+      M.out[gi] = val;
     }
   }
   if (bad) atomicOr(p.nonfinite, 1u);

@@ -370,6 +370,12 @@ class SSPRK3:
         C.check(L.dgsem_ssprk3_stage(h, 3, _ptr(sol.u), _ptr(self.tmp2.u), _ptr(sol.u), t, dt),
                 "stage 3")
 
+    def solve_steps(self, solver: StructuredSolver, sol: Solution, dt: float, nsteps: int) -> None:
+        for _ in range(nsteps):
+            self.step(solver, sol, dt)
+            self.time += dt
+            self.iter += 1
+
     def solve(self, solver: StructuredSolver, sol: Solution, dt: float) -> None:
         """integrator_base.hpp:21-40: fixed dt until final_time, NaN stops."""
         while self.time < self.final_time:
@@ -383,3 +389,115 @@ class SSPRK3:
             except C.DgsemError:
                 self.has_nan = True
                 break
+
+
+# ---------------------------------------------------------------- batched mode
+class BatchSolver:
+    """Many independent periodic meshes (uneven sizes and degrees) sharing one
+    scheme, advanced together (dgsem_batch_* in include/dgsem_b200.h).
+
+    `meshes` is a list of (StructuredMesh, polydeg); the states of all meshes
+    live in one device array `u` of length offsets[-1]; mesh m's state is
+    u[offsets[m]:offsets[m+1]] in the single-mesh layout.
+    """
+
+    def __init__(self, equations, meshes, volume_flux=ChandrashekarFlux,
+                 surface_flux=LaxFriedrichsFlux, stream: torch.cuda.Stream | None = None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("BatchSolver needs a CUDA device (no CPU path)")
+        self.eq = equations
+        self.meshes = list(meshes)
+        n = len(self.meshes)
+        arr = (C.MeshDesc * n)()
+        for k, (mesh, N) in enumerate(self.meshes):
+            d = arr[k]
+            d.ndims = mesh.ndims
+            d.polydeg = int(N)
+            for a in range(3):
+                d.n_cells[a] = int(mesh.n_cells[a]) if a < mesh.ndims else 1
+                d.domain_left[a] = float(mesh.domain_left[a]) if a < mesh.ndims else 0.0
+                d.domain_right[a] = float(mesh.domain_right[a]) if a < mesh.ndims else 1.0
+        s = C.SchemeDesc()
+        s.equation = equations.code
+        s.volume_flux = volume_flux.code
+        s.surface_flux = surface_flux.code
+        s.volume_integral = C.VI_SPLIT_FORM
+        s.gamma = equations.gamma
+        s.alpha_max, s.alpha_min = 0.5, 0.001
+        self.stream = stream or torch.cuda.current_stream()
+        h = ctypes.c_void_p()
+        C.check(C.lib().dgsem_batch_create(arr, n, ctypes.byref(s),
+                                           ctypes.c_void_p(self.stream.cuda_stream),
+                                           ctypes.byref(h)), "dgsem_batch_create")
+        self._h = h
+        offs = (ctypes.c_int64 * (n + 1))()
+        C.check(C.lib().dgsem_batch_offsets(h, offs), "dgsem_batch_offsets")
+        self.offsets = list(offs)
+        self.u = torch.zeros(self.offsets[-1], dtype=torch.float64,
+                             device=torch.device("cuda", torch.cuda.current_device()))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            C.lib().dgsem_batch_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def mesh_state(self, m: int, u: torch.Tensor | None = None) -> torch.Tensor:
+        mesh, N = self.meshes[m]
+        u = self.u if u is None else u
+        nodes = (N + 1) ** mesh.ndims
+        return u[self.offsets[m]:self.offsets[m + 1]].view(mesh.get_nelem(),
+                                                            self.eq.NVARS, nodes)
+
+    def initialize(self, kind: int, params=None) -> None:
+        arr = None
+        if params is not None:
+            flat = [float(x) for p in params for x in p]
+            arr = (ctypes.c_double * len(flat))(*flat)
+        C.check(C.lib().dgsem_batch_initial_condition(self._h, int(kind), arr,
+                                                      ctypes.c_void_p(self.u.data_ptr())),
+                "dgsem_batch_initial_condition")
+
+    def step(self, t: float, dt, u: torch.Tensor | None = None) -> None:
+        u = self.u if u is None else u
+        dts = (ctypes.c_double * len(self.meshes))(*[float(x) for x in dt])
+        C.check(C.lib().dgsem_batch_ssprk3_step(self._h, ctypes.c_void_p(u.data_ptr()),
+                                                float(t), dts), "dgsem_batch_ssprk3_step")
+
+    def graph(self, dt, nsteps: int, u: torch.Tensor | None = None) -> "BatchGraph":
+        return BatchGraph(self, dt, nsteps, self.u if u is None else u)
+
+    def check_finite(self) -> None:
+        C.check(C.lib().dgsem_batch_check_finite(self._h), "dgsem_batch_check_finite")
+
+    def launch_count(self) -> int:
+        c = ctypes.c_int64()
+        C.check(C.lib().dgsem_batch_launch_count(self._h, ctypes.byref(c)),
+                "dgsem_batch_launch_count")
+        return c.value
+
+
+class BatchGraph:
+    """CUDA graph of `nsteps` batched SSPRK3 steps (replayed with launch())."""
+
+    def __init__(self, batch: BatchSolver, dt, nsteps: int, u: torch.Tensor):
+        self.batch = batch
+        dts = (ctypes.c_double * len(batch.meshes))(*[float(x) for x in dt])
+        g = ctypes.c_void_p()
+        C.check(C.lib().dgsem_batch_graph_create(batch.handle, ctypes.c_void_p(u.data_ptr()),
+                                                 dts, int(nsteps), ctypes.byref(g)),
+                "dgsem_batch_graph_create")
+        self._g = g
+
+    def launch(self) -> None:
+        C.check(C.lib().dgsem_batch_graph_launch(self._g), "dgsem_batch_graph_launch")
+
+    def __del__(self):
+        g = getattr(self, "_g", None)
+        if g is not None and g.value:
+            C.lib().dgsem_batch_graph_destroy(g)
+            self._g = None

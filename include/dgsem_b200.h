@@ -177,6 +177,38 @@ dgsem_status dgsem_graph_create(dgsem_ctx* ctx, double* u, double dt,
 dgsem_status dgsem_graph_launch(dgsem_graph* g, double t0);
 dgsem_status dgsem_graph_destroy(dgsem_graph* g);
 
+/* ---------------------------------------------------------------------
+ * Batched mode (no counterpart in the reference, which advances one mesh per
+ * solver instance): n_meshes independent periodic meshes sharing one scheme
+ * (Euler, split form), each with its own degree, element counts and domain.
+ * The states of all meshes live in one device array; mesh m occupies
+ * [offsets[m], offsets[m+1]) in the single-mesh layout.  Per stage one fused
+ * launch per distinct degree, the degrees running concurrently.
+ * --------------------------------------------------------------------- */
+typedef struct dgsem_batch dgsem_batch;
+typedef struct dgsem_batch_graph dgsem_batch_graph;
+dgsem_status dgsem_batch_create(const dgsem_mesh_desc* meshes, int n_meshes,
+                                const dgsem_scheme_desc* scheme, void* stream,
+                                dgsem_batch** out);
+dgsem_status dgsem_batch_destroy(dgsem_batch* b);
+/* offsets: n_meshes + 1 entries (doubles). */
+dgsem_status dgsem_batch_offsets(const dgsem_batch* b, int64_t* offsets);
+/* params: 3 doubles per mesh (see dgsem_initial_kind) or NULL. */
+dgsem_status dgsem_batch_initial_condition(dgsem_batch* b, int kind,
+                                           const double* params, double* u);
+/* One SSPRK3 step of every mesh; dt_host[m] is mesh m's time step. */
+dgsem_status dgsem_batch_ssprk3_step(dgsem_batch* b, double* u, double t,
+                                     const double* dt_host);
+/* CUDA graph of nsteps batched steps (3 * nsteps * n_degrees launches, the
+ * degrees as parallel branches); replay on the batch's stream. */
+dgsem_status dgsem_batch_graph_create(dgsem_batch* b, double* u,
+                                      const double* dt_host, int nsteps,
+                                      dgsem_batch_graph** out);
+dgsem_status dgsem_batch_graph_launch(dgsem_batch_graph* g);
+dgsem_status dgsem_batch_graph_destroy(dgsem_batch_graph* g);
+dgsem_status dgsem_batch_check_finite(dgsem_batch* b);
+dgsem_status dgsem_batch_launch_count(const dgsem_batch* b, int64_t* count);
+
 /* Hennemann-Gassner blending factor per element and troubled-cell flag
  * (alpha > max(100 eps, eps^0.75), volume_flux.hpp:772-773).  Either output
  * may be NULL. */
