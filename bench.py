@@ -285,6 +285,11 @@ def run_device_arm(args):
     dt = time_step_size(name)
     solver, sol = build_solver(name, dev)
     integ = D.SSPRK3(sol, solver.mesh, 0.0)
+    if args.variant == "auto":
+        variant, variant_ms = solver.autotune(sol.u, retime=True)
+    else:
+        variant, variant_ms = int(args.variant), None
+        solver.set_launch_variant(variant)
     stream = solver.stream
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     L = C.lib()
@@ -378,7 +383,8 @@ def run_device_arm(args):
         "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (analytic initial condition of the workload)",
         "config": dict(workload_config(name),
-                       parallelism=("replicas" if world > 1 else "single")),
+                       parallelism=("replicas" if world > 1 else "single"),
+                       launch_variant=variant, variant_ms=variant_ms),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs"
@@ -446,6 +452,7 @@ def run_batched(args):
     batch = D.BatchSolver(eq, meshes, D.ChandrashekarFlux, D.LaxFriedrichsFlux)
     batch.initialize(C.IC_ISENTROPIC_VORTEX, [(b, c[0], c[1]) for _, _, b, c in specs])
     stream = batch.stream
+    variants = batch.autotune(dts) if args.variant == "auto" else None
     g = batch.graph(dts, 1)
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
@@ -478,6 +485,8 @@ def run_batched(args):
                                     stream=stream)
         sol = D.Solution(mesh, basis, eq, device=dev)
         solver.initialize(D.IsentropicVortex(beta, c), sol)
+        if args.variant == "auto":
+            solver.autotune(sol.u)
         integ = D.SSPRK3(sol, mesh, 0.0)
         with torch.cuda.stream(stream):
             integ.solve_steps(solver, sol, dts[k], 2)
@@ -512,7 +521,8 @@ def run_batched(args):
                    "degrees": sorted({N for _, N, _, _ in specs}),
                    "volume_flux": "chandrashekar", "surface_flux": "llf",
                    "l2": "inputs larger than L2 (state %.2f GB)" % (dofs * 32 / 1e9),
-                   "graph": "one SSPRK3 step per graph replay; degrees as parallel branches"},
+                   "graph": "one SSPRK3 step per graph replay; degrees as parallel branches",
+                   "launch_variants": variants},
         "speedup_vs_per_instance": plain_ms / batched_ms,
         "per_instance_ms_per_step_sum": plain_ms,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -535,6 +545,8 @@ def main():
     ap.add_argument("--workload", default="tgv16", choices=list(WORKLOADS) + ["batched"])
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--variant", default="auto", choices=["auto", "0", "1", "2"],
+                    help="launch shape of the stage kernel (auto = autotuned)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

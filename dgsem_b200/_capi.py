@@ -38,7 +38,8 @@ EXPORTED = [
     "dgsem_batch_create", "dgsem_batch_destroy", "dgsem_batch_offsets",
     "dgsem_batch_initial_condition", "dgsem_batch_ssprk3_step", "dgsem_batch_graph_create",
     "dgsem_batch_graph_launch", "dgsem_batch_graph_destroy", "dgsem_batch_check_finite",
-    "dgsem_batch_launch_count",
+    "dgsem_batch_launch_count", "dgsem_autotune", "dgsem_set_launch_variant",
+    "dgsem_batch_autotune",
 ]
 
 
@@ -114,6 +115,9 @@ def lib() -> ctypes.CDLL:
     L.dgsem_batch_graph_destroy.argtypes = [vp]
     L.dgsem_batch_check_finite.argtypes = [vp]
     L.dgsem_batch_launch_count.argtypes = [vp, c.POINTER(c.c_int64)]
+    L.dgsem_autotune.argtypes = [vp, dp, c.POINTER(c.c_int), c.POINTER(c.c_double)]
+    L.dgsem_set_launch_variant.argtypes = [vp, c.c_int]
+    L.dgsem_batch_autotune.argtypes = [vp, dp, c.POINTER(c.c_double), c.POINTER(c.c_int)]
     for name in EXPORTED:
         f = getattr(L, name)
         if name != "dgsem_status_string":

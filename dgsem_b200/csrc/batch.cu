@@ -28,6 +28,7 @@ struct Group {
   int n = 0;                      // nodes per direction
   std::unique_ptr<EngineBase> engine;
   EngineConfig cfg{};
+  std::vector<int> members;       // mesh indices of this degree
   int ntiles = 0;
   int* tile_mesh = nullptr;       // device
   int* tile_e0 = nullptr;         // device
@@ -90,6 +91,9 @@ void bfree(dgsem_batch* b) {
 
 dgsem_status st_of(cudaError_t e) { return e == cudaSuccess ? DGSEM_OK : DGSEM_ERR_CUDA; }
 
+// (Re)builds a group's tile list for its engine's current launch shape.
+cudaError_t build_tiles(const dgsem_batch* b, Group& g);
+
 // Per-stage mesh views for state u (stages: u -> tmp1 -> tmp2 -> u) and the
 // per-mesh time steps; uploaded only when u or dt changes.
 dgsem_status upload_views(dgsem_batch* b, double* u, const double* dt) {
@@ -146,9 +150,68 @@ dgsem_status launch_stage(dgsem_batch* b, int stage, double t, const double* t_d
   return DGSEM_OK;
 }
 
+cudaError_t build_tiles(const dgsem_batch* b, Group& g) {
+  const int epb = g.engine->elements_per_block();
+  std::vector<int> tm, te;
+  for (int m : g.members)
+    for (int64_t e0 = 0; e0 < b->nelem[m]; e0 += epb) {
+      tm.push_back(m);
+      te.push_back((int)e0);
+    }
+  g.ntiles = (int)tm.size();
+  cudaError_t e = cudaMemcpy(g.tile_mesh, tm.data(), tm.size() * sizeof(int),
+                             cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(g.tile_e0, te.data(), te.size() * sizeof(int), cudaMemcpyHostToDevice);
+  return e;
+}
+
 }  // namespace
 
 extern "C" {
+
+dgsem_status dgsem_batch_autotune(dgsem_batch* b, double* u, const double* dt_host,
+                                  int* chosen) {
+  if (!b || !u || !dt_host) return DGSEM_ERR_INVALID_ARG;
+  dgsem_status st = upload_views(b, u, dt_host);
+  if (st != DGSEM_OK) return st;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int gi = 0;
+  for (Group& g : b->groups) {
+    int best = 0;
+    float best_ms = 1e30f;
+    for (int v = 0; v < kNumVariants && st == DGSEM_OK; ++v) {
+      g.engine->set_variant(v);
+      if (build_tiles(b, g) != cudaSuccess) st = DGSEM_ERR_CUDA;
+      // stage 1 writes tmp1 only, so repeated launches leave u untouched
+      auto run = [&]() {
+        return g.engine->batch_stage(g.cfg, b->views, g.tile_mesh, g.tile_e0, g.ntiles, 0.0,
+                                     1.0, 0.0, nullptr, b->stream);
+      };
+      if (st == DGSEM_OK && run() != cudaSuccess) st = DGSEM_ERR_CUDA;
+      cudaEventRecord(e0, b->stream);
+      for (int r = 0; r < 3 && st == DGSEM_OK; ++r)
+        if (run() != cudaSuccess) st = DGSEM_ERR_CUDA;
+      cudaEventRecord(e1, b->stream);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = v;
+      }
+    }
+    g.engine->set_variant(best);
+    if (st == DGSEM_OK && build_tiles(b, g) != cudaSuccess) st = DGSEM_ERR_CUDA;
+    if (chosen) chosen[gi] = best;
+    ++gi;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return st;
+}
 
 dgsem_status dgsem_batch_create(const dgsem_mesh_desc* meshes, int n_meshes,
                                 const dgsem_scheme_desc* scheme, void* stream,
@@ -267,25 +330,21 @@ dgsem_status dgsem_batch_create(const dgsem_mesh_desc* meshes, int n_meshes,
     c.nonfinite = b->flag;
     c.grad = nullptr;
     for (int f = 0; f < 6; ++f) c.bc.kind[f] = 0;
-    const int epb = g.engine->elements_per_block();
-    std::vector<int> tm, te;
-    for (int m : kv.second)
-      for (int64_t e0 = 0; e0 < b->nelem[m]; e0 += epb) {
-        tm.push_back(m);
-        te.push_back((int)e0);
-      }
-    g.ntiles = (int)tm.size();
-    g.tile_mesh = balloc<int>(b, tm.size());
-    g.tile_e0 = balloc<int>(b, te.size());
+    g.members = kv.second;
+    // tile arrays sized for the smallest elements-per-block shape
+    g.engine->set_variant(0);
+    size_t max_tiles = 0;
+    for (int m : g.members)
+      max_tiles += (b->nelem[m] + g.engine->elements_per_block() - 1) /
+                   g.engine->elements_per_block();
+    g.tile_mesh = balloc<int>(b, max_tiles);
+    g.tile_e0 = balloc<int>(b, max_tiles);
     if (!g.tile_mesh || !g.tile_e0) {
       bfree(b);
       delete b;
       return DGSEM_ERR_ALLOC;
     }
-    if (e == cudaSuccess)
-      e = cudaMemcpy(g.tile_mesh, tm.data(), tm.size() * sizeof(int), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess)
-      e = cudaMemcpy(g.tile_e0, te.data(), te.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = build_tiles(b, g);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming);
     b->groups.push_back(std::move(g));

@@ -4,10 +4,16 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <limits>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <new>
+#include <sstream>
+#include <string>
 #include <vector>
 
 #include "../../include/dgsem_b200.h"
@@ -645,6 +651,125 @@ dgsem_status dgsem_check_finite(dgsem_ctx* ctx) {
 dgsem_status dgsem_launch_count(const dgsem_ctx* ctx, int64_t* count) {
   if (!ctx || !count) return DGSEM_ERR_INVALID_ARG;
   *count = ctx->launches;
+  return DGSEM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Launch-shape autotuner: every engine has kNumVariants launch shapes of the
+// same kernel (bitwise-identical results).  Tuning times each on the real mesh
+// and state; choices are cached per (scheme, degree, element count) for the
+// process and, if DGSEM_TUNING_FILE names a file, persisted there as lines
+// "key variant".
+// ---------------------------------------------------------------------------
+namespace dgsem {
+namespace tune_detail {
+
+std::mutex& tune_mutex() {
+  static std::mutex m;
+  return m;
+}
+
+std::map<std::string, int>& tune_cache() {
+  static std::map<std::string, int> cache;
+  static bool loaded = false;
+  if (!loaded) {
+    loaded = true;
+    if (const char* path = std::getenv("DGSEM_TUNING_FILE")) {
+      std::ifstream in(path);
+      std::string key;
+      int v;
+      while (in >> key >> v)
+        if (v >= 0 && v < kNumVariants) cache[key] = v;
+    }
+  }
+  return cache;
+}
+
+void tune_store(const std::string& key, int v) {
+  tune_cache()[key] = v;
+  if (const char* path = std::getenv("DGSEM_TUNING_FILE")) {
+    std::ofstream out(path, std::ios::app);
+    out << key << " " << v << "\n";
+  }
+}
+
+}  // namespace tune_detail
+
+std::string tune_key(int ndims, int n, int vf, int sf, int hg, int ns, int64_t nelem) {
+  std::ostringstream k;
+  k << "d" << ndims << "_n" << n << "_vf" << vf << "_sf" << sf << "_hg" << hg << "_ns" << ns
+    << "_e" << nelem;
+  return k.str();
+}
+
+// Times `launch` (one kernel launch sequence on `s`) for each variant of
+// `eng`; returns the fastest variant and optionally the mean times.
+template <class Launch>
+int time_variants(EngineBase* eng, cudaStream_t s, Launch&& launch, double* times_ms) {
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  int best = 0;
+  float best_ms = 1e30f;
+  for (int v = 0; v < kNumVariants; ++v) {
+    eng->set_variant(v);
+    launch();  // warm-up
+    cudaEventRecord(a, s);
+    constexpr int reps = 5;
+    for (int r = 0; r < reps; ++r) launch();
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    ms /= reps;
+    if (times_ms) times_ms[v] = ms;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = v;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return best;
+}
+
+}  // namespace dgsem
+
+extern "C" {
+
+dgsem_status dgsem_set_launch_variant(dgsem_ctx* ctx, int variant) {
+  if (!ctx || variant < 0 || variant >= kNumVariants) return DGSEM_ERR_INVALID_ARG;
+  ctx->engine->set_variant(variant);
+  return DGSEM_OK;
+}
+
+dgsem_status dgsem_autotune(dgsem_ctx* ctx, const double* u, int* chosen, double* times_ms) {
+  using namespace dgsem::tune_detail;
+  if (!ctx || !u) return DGSEM_ERR_INVALID_ARG;
+  const EngineConfig& c = ctx->cfg;
+  const std::string key =
+      tune_key(c.ndims, c.n, ctx->scheme.volume_flux, ctx->scheme.surface_flux,
+               ctx->scheme.volume_integral, ctx->scheme.equation == DGSEM_NAVIER_STOKES_2D,
+               c.nelem);
+  std::lock_guard<std::mutex> lock(tune_mutex());
+  auto it = tune_cache().find(key);
+  if (it != tune_cache().end() && !times_ms) {
+    ctx->engine->set_variant(it->second);
+    if (chosen) *chosen = it->second;
+    return DGSEM_OK;
+  }
+  cudaError_t err = cudaSuccess;
+  const int best = time_variants(ctx->engine.get(), ctx->stream, [&]() {
+    cudaError_t e = ctx->engine->stage(ctx->cfg, nullptr, u, ctx->tmp1, 0.0, 0.0, 1.0, 0.0,
+                                       nullptr, nullptr, ctx->stream);
+    if (e != cudaSuccess) err = e;
+  }, times_ms);
+  if (err != cudaSuccess) return DGSEM_ERR_CUDA;
+  ctx->engine->set_variant(best);
+  tune_store(key, best);
+  if (chosen) *chosen = best;
   return DGSEM_OK;
 }
 

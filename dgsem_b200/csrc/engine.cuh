@@ -1,6 +1,9 @@
 // Type-erased solver engine: one instantiation per supported template
 // combination (dimension, nodes per direction, volume flux, surface flux,
-// shock capturing).  The C ABI context owns one engine.
+// shock capturing, Navier-Stokes).  Each engine carries several launch shapes
+// of the same fused kernel (elements per block, register cap); they compute
+// bitwise-identical results and the autotuner (capi.cu: dgsem_autotune)
+// picks the fastest for a mesh.  The C ABI context owns one engine.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -32,6 +35,8 @@ struct EngineConfig {
   double* grad;             // Navier-Stokes lifted gradient [E][4][2][n^2]
 };
 
+constexpr int kNumVariants = 3;
+
 class EngineBase {
  public:
   virtual ~EngineBase() = default;
@@ -42,7 +47,7 @@ class EngineBase {
                             double* alpha_out, cudaStream_t s) = 0;
   // Batched launch over a tile list (mesh index and first element per block)
   // of meshes sharing this engine's scheme and degree; per-mesh data in
-  // `meshes` (device array).
+  // `meshes` (device array).  Tiles are built with elements_per_block().
   virtual cudaError_t batch_stage(const EngineConfig& cfg, const MeshView* meshes,
                                   const int* tile_mesh, const int* tile_e0, int ntiles,
                                   double a, double b, double t, const double* t_dev,
@@ -51,6 +56,9 @@ class EngineBase {
   virtual int elements_per_block() const = 0;
   virtual int threads_per_block() const = 0;
   virtual size_t smem_bytes() const = 0;
+  // launch-shape variant in [0, kNumVariants)
+  virtual void set_variant(int v) = 0;
+  virtual int variant() const = 0;
 };
 
 std::unique_ptr<EngineBase> make_engine(int ndims, int n, int vf, int sf,
@@ -75,32 +83,61 @@ inline void fill_basis_const(const BasisTables& b, BasisConst<N>* out) {
   out->lhat_rN = b.lhat_right[N - 1];
 }
 
-// Launch geometry per (DIM, N): one thread per element line.
-template <int DIM, int N>
+// Launch geometry per (DIM, N, variant): one thread per element line.
+//   variant 0: ~128 (2D) / ~96 (3D) threads per block, no register cap
+//   variant 1: same block, register cap for one more resident block per SM
+//   variant 2: twice the elements per block, no register cap
+template <int DIM, int N, int V>
 struct LaunchShape {
   static constexpr int NLINE = DIM * ipow(N, DIM - 1);
   static constexpr int TARGET = DIM == 2 ? 128 : 96;
-  static constexpr int EPB = (TARGET / NLINE) > 0 ? (TARGET / NLINE) : 1;
+  static constexpr int EPB0 = (TARGET / NLINE) > 0 ? (TARGET / NLINE) : 1;
+  static constexpr int EPB = V == 2 ? 2 * EPB0 : EPB0;
   static constexpr int NT = ((EPB * NLINE + 31) / 32) * 32;
+  // variant 1 caps registers at 65536 / (MINB * NT) (about 100 per thread);
+  // MINB = 0: no cap
+  static constexpr int MINB = V == 1 ? (65536 / (NT * 100) > 1 ? 65536 / (NT * 100) : 2) : 0;
 };
 
 template <int DIM, int N, int VF, int SF, bool HG, bool NS = false>
 class Engine final : public EngineBase {
  public:
-  using L = LaunchShape<DIM, N>;
-  static constexpr int EPB = L::EPB;
-  static constexpr int NT = L::NT;
-  using Shape = StageShape<DIM, N, VF, SF, HG, EPB, NS>;
   static constexpr int GRAD_EPB = (128 / (N * N)) > 0 ? (128 / (N * N)) : 1;
+  static constexpr bool kBatch = !NS && !HG;
+
+  template <int V>
+  using Sh = StageShape<DIM, N, VF, SF, HG, LaunchShape<DIM, N, V>::EPB, NS>;
+
+  template <int V>
+  static auto kernel() {
+    using L = LaunchShape<DIM, N, V>;
+    if constexpr (L::MINB == 0)
+      return stage_kernel<DIM, N, VF, SF, HG, L::EPB, L::NT, NS, false>;
+    else
+      return stage_kernel_capped<DIM, N, VF, SF, HG, L::EPB, L::NT, NS, false, L::MINB>;
+  }
+  template <int V>
+  static auto batch_kernel() {
+    using L = LaunchShape<DIM, N, V>;
+    if constexpr (L::MINB == 0)
+      return stage_kernel<DIM, N, VF, SF, HG, L::EPB, L::NT, NS, true>;
+    else
+      return stage_kernel_capped<DIM, N, VF, SF, HG, L::EPB, L::NT, NS, true, L::MINB>;
+  }
+
+  template <int V>
+  static void set_attributes() {
+    cudaFuncSetAttribute(kernel<V>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)Sh<V>::smem_bytes);
+    if constexpr (kBatch)
+      cudaFuncSetAttribute(batch_kernel<V>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)Sh<V>::smem_bytes);
+  }
 
   Engine() {
-    cudaFuncSetAttribute(stage_kernel<DIM, N, VF, SF, HG, EPB, NT, NS>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)Shape::smem_bytes);
-    if constexpr (!NS && !HG)
-      cudaFuncSetAttribute(stage_kernel<DIM, N, VF, SF, HG, EPB, NT, NS, true>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)Shape::smem_bytes);
+    set_attributes<0>();
+    set_attributes<1>();
+    set_attributes<2>();
   }
 
   StageArgs<N> common_args(const EngineConfig& cfg, double a, double b, double t,
@@ -125,6 +162,13 @@ class Engine final : public EngineBase {
     args.bc = cfg.bc;
     fill_basis_const<N>(cfg.basis, &args.basis);
     return args;
+  }
+
+  template <int V>
+  void launch(const StageArgs<N>& args, int64_t nelem, cudaStream_t s) const {
+    using L = LaunchShape<DIM, N, V>;
+    const int64_t blocks = (nelem + L::EPB - 1) / L::EPB;
+    kernel<V>()<<<(unsigned)blocks, L::NT, Sh<V>::smem_bytes, s>>>(args);
   }
 
   cudaError_t stage(const EngineConfig& cfg, const double* u_n,
@@ -155,32 +199,57 @@ class Engine final : public EngineBase {
       br1_gradient_kernel<N, GRAD_EPB>
           <<<(unsigned)gblocks, GRAD_EPB * N * N, 0, s>>>(ga);
     }
-    const int64_t blocks = (cfg.nelem + EPB - 1) / EPB;
-    stage_kernel<DIM, N, VF, SF, HG, EPB, NT, NS>
-        <<<(unsigned)blocks, NT, Shape::smem_bytes, s>>>(args);
+    switch (variant_) {
+      case 1: launch<1>(args, cfg.nelem, s); break;
+      case 2: launch<2>(args, cfg.nelem, s); break;
+      default: launch<0>(args, cfg.nelem, s); break;
+    }
     return cudaGetLastError();
+  }
+
+  template <int V>
+  void launch_batch(const StageArgs<N>& args, int ntiles, cudaStream_t s) const {
+    if constexpr (kBatch) {
+      using L = LaunchShape<DIM, N, V>;
+      batch_kernel<V>()<<<(unsigned)ntiles, L::NT, Sh<V>::smem_bytes, s>>>(args);
+    }
   }
 
   cudaError_t batch_stage(const EngineConfig& cfg, const MeshView* meshes,
                           const int* tile_mesh, const int* tile_e0, int ntiles,
                           double a, double b, double t, const double* t_dev,
                           cudaStream_t s) override {
-    if constexpr (NS || HG) {
+    if constexpr (!kBatch) {
       return cudaErrorNotSupported;
     } else {
       StageArgs<N> args = common_args(cfg, a, b, t, t_dev, nullptr);
       args.meshes = meshes;
       args.tile_mesh = tile_mesh;
       args.tile_e0 = tile_e0;
-      stage_kernel<DIM, N, VF, SF, HG, EPB, NT, NS, true>
-          <<<(unsigned)ntiles, NT, Shape::smem_bytes, s>>>(args);
+      switch (variant_) {
+        case 1: launch_batch<1>(args, ntiles, s); break;
+        case 2: launch_batch<2>(args, ntiles, s); break;
+        default: launch_batch<0>(args, ntiles, s); break;
+      }
       return cudaGetLastError();
     }
   }
+
   int kernels_per_stage() const override { return NS ? 2 : 1; }
-  int elements_per_block() const override { return EPB; }
-  int threads_per_block() const override { return NT; }
-  size_t smem_bytes() const override { return Shape::smem_bytes; }
+  int elements_per_block() const override {
+    return variant_ == 2 ? LaunchShape<DIM, N, 2>::EPB : LaunchShape<DIM, N, 0>::EPB;
+  }
+  int threads_per_block() const override {
+    return variant_ == 2 ? LaunchShape<DIM, N, 2>::NT : LaunchShape<DIM, N, 0>::NT;
+  }
+  size_t smem_bytes() const override {
+    return variant_ == 2 ? Sh<2>::smem_bytes : Sh<0>::smem_bytes;
+  }
+  void set_variant(int v) override { variant_ = (v >= 0 && v < kNumVariants) ? v : 0; }
+  int variant() const override { return variant_; }
+
+ private:
+  int variant_ = 0;
 };
 
 }  // namespace dgsem

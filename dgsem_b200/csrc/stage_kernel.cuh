@@ -68,9 +68,9 @@ struct BcParams {
   double sqrt3;
 };
 
-// Per-mesh data of one stage launch.  A block stages its mesh's view into
-// shared memory at start: single-mesh launches copy it from the kernel
-// parameters, batched launches from the per-tile mesh list.
+// Per-mesh data of one stage launch.  Single-mesh launches read it from the
+// kernel parameters; in batched launches each block copies its mesh's view
+// from the per-tile mesh list into shared memory at start.
 struct MeshView {
   const double* u_in;
   const double* u_n;
@@ -621,10 +621,10 @@ __device__ __forceinline__ void process_line(const StageArgs<N>& p, const MeshVi
   }
 }
 
-template <int DIM, int N, int VF, int SF, bool HG, int EPB, int NT, bool NS = false,
-          bool BATCH = false>
-__global__ void __launch_bounds__(NT)
-    stage_kernel(const StageArgs<N> p) {
+// Body of the fused stage kernel; the two __global__ wrappers below differ
+// only in their launch bounds.
+template <int DIM, int N, int VF, int SF, bool HG, int EPB, int NT, bool NS, bool BATCH>
+__device__ __forceinline__ void stage_body(const StageArgs<N>& p) {
   using S = StageShape<DIM, N, VF, SF, HG, EPB, NS>;
   using Q = NodeSlots<DIM, VF>;
   static_assert(!NS || (DIM == 2 && !HG), "Navier-Stokes: 2D split form only");
@@ -641,17 +641,19 @@ __global__ void __launch_bounds__(NT)
   int* info = reinterpret_cast<int*>(vinv_s + S::SM_VINV);
 
   const int tid = threadIdx.x;
+  // Batched launches stage the block's mesh view in shared memory; single-mesh
+  // launches read it from the kernel parameters (constant bank), which keeps
+  // the table pointers out of shared-memory loads in the line loop.
   __shared__ MeshView mesh_s;
   int e0;
   if constexpr (BATCH) {
     e0 = p.tile_e0[blockIdx.x];
     if (tid == 0) mesh_s = p.meshes[p.tile_mesh[blockIdx.x]];
+    __syncthreads();
   } else {
     e0 = (int)blockIdx.x * EPB;
-    if (tid == 0) mesh_s = p.mesh;
   }
-  __syncthreads();
-  const MeshView& M = mesh_s;
+  const MeshView& M = BATCH ? mesh_s : p.mesh;
   const int nelem = M.nelem;
   if (e0 >= nelem) return;
   const int ne = min(EPB, nelem - e0);
@@ -835,6 +837,21 @@ __global__ void __launch_bounds__(NT)
     }
   }
   if (bad) atomicOr(p.nonfinite, 1u);
+}
+
+// Fused stage kernel, register allocation left to the compiler.
+template <int DIM, int N, int VF, int SF, bool HG, int EPB, int NT, bool NS = false,
+          bool BATCH = false>
+__global__ void __launch_bounds__(NT) stage_kernel(const StageArgs<N> p) {
+  stage_body<DIM, N, VF, SF, HG, EPB, NT, NS, BATCH>(p);
+}
+
+// Same kernel with MINB resident blocks per SM requested from the register
+// allocator (a register cap of 65536 / (MINB * NT) per thread).
+template <int DIM, int N, int VF, int SF, bool HG, int EPB, int NT, bool NS, bool BATCH,
+          int MINB>
+__global__ void __launch_bounds__(NT, MINB) stage_kernel_capped(const StageArgs<N> p) {
+  stage_body<DIM, N, VF, SF, HG, EPB, NT, NS, BATCH>(p);
 }
 
 }  // namespace dgsem

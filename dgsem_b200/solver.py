@@ -338,6 +338,19 @@ class StructuredSolver:
     def check_finite(self) -> None:
         C.check(C.lib().dgsem_check_finite(self._ctx), "dgsem_check_finite")
 
+    def autotune(self, u: torch.Tensor, retime: bool = False):
+        """Picks the fastest launch shape for this mesh (results are identical
+        across shapes); returns (variant, per-variant ms or None)."""
+        chosen = ctypes.c_int()
+        times = (ctypes.c_double * 3)() if retime else None
+        C.check(C.lib().dgsem_autotune(self._ctx, _ptr(u), ctypes.byref(chosen), times),
+                "dgsem_autotune")
+        return chosen.value, (list(times) if retime else None)
+
+    def set_launch_variant(self, variant: int) -> None:
+        C.check(C.lib().dgsem_set_launch_variant(self._ctx, int(variant)),
+                "dgsem_set_launch_variant")
+
     def launch_count(self) -> int:
         c = ctypes.c_int64()
         C.check(C.lib().dgsem_launch_count(self._ctx, ctypes.byref(c)), "dgsem_launch_count")
@@ -473,6 +486,15 @@ class BatchSolver:
 
     def check_finite(self) -> None:
         C.check(C.lib().dgsem_batch_check_finite(self._h), "dgsem_batch_check_finite")
+
+    def autotune(self, dt, u: torch.Tensor | None = None):
+        u = self.u if u is None else u
+        ndeg = len({N for _, N in self.meshes})
+        chosen = (ctypes.c_int * ndeg)()
+        dts = (ctypes.c_double * len(self.meshes))(*[float(x) for x in dt])
+        C.check(C.lib().dgsem_batch_autotune(self._h, ctypes.c_void_p(u.data_ptr()), dts,
+                                             chosen), "dgsem_batch_autotune")
+        return list(chosen)
 
     def launch_count(self) -> int:
         c = ctypes.c_int64()

@@ -207,6 +207,11 @@ dgsem_status dgsem_batch_graph_create(dgsem_batch* b, double* u,
 dgsem_status dgsem_batch_graph_launch(dgsem_batch_graph* g);
 dgsem_status dgsem_batch_graph_destroy(dgsem_batch_graph* g);
 dgsem_status dgsem_batch_check_finite(dgsem_batch* b);
+/* Autotunes the launch shape of every degree group on the batch's meshes
+ * (stage-1 launches into a batch temporary; u is not modified); chosen
+ * receives one variant per distinct degree (ascending), may be NULL. */
+dgsem_status dgsem_batch_autotune(dgsem_batch* b, double* u, const double* dt_host,
+                                  int* chosen);
 dgsem_status dgsem_batch_launch_count(const dgsem_batch* b, int64_t* count);
 
 /* Hennemann-Gassner blending factor per element and troubled-cell flag
@@ -231,6 +236,20 @@ dgsem_status dgsem_from_reference_layout(dgsem_ctx* ctx, const double* u_ref,
  * NaN/Inf.  This call synchronises the stream, returns DGSEM_ERR_NONFINITE if
  * the flag is set, and clears it. */
 dgsem_status dgsem_check_finite(dgsem_ctx* ctx);
+
+/* Launch-shape autotuner (no reference counterpart; the reference has one
+ * fixed Kokkos launch shape).  The fused stage kernel has kNumVariants = 3
+ * launch shapes (elements per block, register cap) with bitwise-identical
+ * results.  dgsem_autotune times each on this context's mesh with state u
+ * (RHS launches into a context temporary; u is not modified), keeps the
+ * fastest and returns it in *chosen (may be NULL); times_ms (3 doubles, may
+ * be NULL) receives the mean launch times and forces re-timing.  Choices are
+ * cached per (scheme, degree, element count) for the process and, when the
+ * environment variable DGSEM_TUNING_FILE names a file, persisted there.
+ * Synchronous. */
+dgsem_status dgsem_autotune(dgsem_ctx* ctx, const double* u, int* chosen,
+                            double* times_ms);
+dgsem_status dgsem_set_launch_variant(dgsem_ctx* ctx, int variant);
 
 /* Number of kernel launches issued by this context so far (diagnostics). */
 dgsem_status dgsem_launch_count(const dgsem_ctx* ctx, int64_t* count);

@@ -90,3 +90,21 @@ def test_batched_mesh_matches_oracle(cuda):
     u1_o = do.ssprk3_step(s, u0, 0.0, dt)
     assert rel_linf(u1, u1_o) <= RTOL
     assert np.isfinite(u1).all()
+
+
+def test_batched_autotune_keeps_results(cuda):
+    import torch
+    a = _batch(cuda)
+    b = _batch(cuda)
+    dts = [1.5e-3] * len(SPECS)
+    u_before = b.u.clone()
+    chosen = b.autotune(dts)
+    torch.cuda.synchronize()
+    assert len(chosen) == len({N for _, N, _, _ in SPECS})
+    assert all(v in (0, 1, 2) for v in chosen)
+    assert torch.equal(b.u, u_before)
+    for s in range(2):
+        a.step(s * dts[0], dts)
+        b.step(s * dts[0], dts)
+    torch.cuda.synchronize()
+    assert torch.equal(a.u, b.u)
