@@ -15,7 +15,10 @@ LIB_PATH = os.path.join(HERE, "_lib", "libdgsem_b200.so")
 DGSEM_OK = 0
 STATUS_NAMES = {0: "ok", 1: "invalid argument", 2: "unsupported combination",
                 3: "CUDA error", 4: "non-finite value in state",
-                5: "device wait timed out", 6: "allocation failed"}
+                5: "device wait timed out", 6: "allocation failed",
+                7: "state larger than the static scratch"}
+DGSEM_ERR_SCRATCH_LIMIT = 7
+STATIC_SCRATCH_MAX_STATE = 2097152  # DGSEM_STATIC_SCRATCH_MAX_STATE (doubles per stage state)
 
 # enums (include/dgsem_b200.h)
 EULER_2D, EULER_3D, NAVIER_STOKES_2D = 0, 1, 2
@@ -39,7 +42,7 @@ EXPORTED = [
     "dgsem_batch_initial_condition", "dgsem_batch_ssprk3_step", "dgsem_batch_graph_create",
     "dgsem_batch_graph_launch", "dgsem_batch_graph_destroy", "dgsem_batch_check_finite",
     "dgsem_batch_launch_count", "dgsem_autotune", "dgsem_set_launch_variant",
-    "dgsem_batch_autotune",
+    "dgsem_batch_autotune", "dgsem_ssprk3_step_static_scratch",
 ]
 
 
@@ -118,6 +121,7 @@ def lib() -> ctypes.CDLL:
     L.dgsem_autotune.argtypes = [vp, dp, c.POINTER(c.c_int), c.POINTER(c.c_double)]
     L.dgsem_set_launch_variant.argtypes = [vp, c.c_int]
     L.dgsem_batch_autotune.argtypes = [vp, dp, c.POINTER(c.c_double), c.POINTER(c.c_int)]
+    L.dgsem_ssprk3_step_static_scratch.argtypes = [vp, dp, c.c_double, c.c_double]
     for name in EXPORTED:
         f = getattr(L, name)
         if name != "dgsem_status_string":

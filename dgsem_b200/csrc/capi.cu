@@ -243,6 +243,7 @@ const char* dgsem_status_string(dgsem_status s) {
     case DGSEM_ERR_NONFINITE: return "non-finite value in state";
     case DGSEM_ERR_TIMEOUT: return "device wait timed out";
     case DGSEM_ERR_ALLOC: return "allocation failed";
+    case DGSEM_ERR_SCRATCH_LIMIT: return "state larger than the static scratch";
   }
   return "unknown status";
 }

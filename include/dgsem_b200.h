@@ -49,7 +49,8 @@ typedef enum dgsem_status {
   DGSEM_ERR_CUDA = 3,
   DGSEM_ERR_NONFINITE = 4,
   DGSEM_ERR_TIMEOUT = 5,
-  DGSEM_ERR_ALLOC = 6
+  DGSEM_ERR_ALLOC = 6,
+  DGSEM_ERR_SCRATCH_LIMIT = 7  /* state larger than the static scratch */
 } dgsem_status;
 
 typedef enum dgsem_equation {
@@ -159,6 +160,33 @@ dgsem_status dgsem_ssprk3_step(dgsem_ctx* ctx, double* u, double t, double dt);
 /* nsteps SSPRK3 steps in place, t_k = t0 + k*dt. */
 dgsem_status dgsem_ssprk3_steps(dgsem_ctx* ctx, double* u, double t0,
                                 double dt, int nsteps);
+
+/* One SSPRK3 step in place that allocates nothing (no counterpart in the
+ * reference, whose integrator owns its stage Views).  Same kernels and the
+ * same result as dgsem_ssprk3_step, but the two stage states live in one
+ * static device array of this library instead of the context's temporaries.
+ * For callers that must not allocate or free device memory while stepping:
+ * a host code whose memory manager holds the GPU's memory in its own pool
+ * (a cudaMalloc could fail or fragment it) or that cannot take the
+ * device-wide synchronisation a cudaFree may bring; and for many small
+ * contexts on one device that step one after another through one scratch.
+ *  - Limit: the state may hold at most DGSEM_STATIC_SCRATCH_MAX_STATE doubles
+ *    (2^21, 16 MiB; the scratch is 2 x 16 MiB per device); larger states
+ *    return DGSEM_ERR_SCRATCH_LIMIT and launch nothing.
+ *  - u must be device memory of the CURRENT device (else
+ *    DGSEM_ERR_INVALID_ARG), and the context must belong to that device.
+ *  - The first call on a device is its set-up: it looks up the scratch's
+ *    address (cudaGetSymbolAddress, which may load the module that holds
+ *    the scratch).  Make that first call before any stream capture.
+ *  - Nothing has to start at zero: each stage state is fully written before
+ *    it is read.
+ *  - There is ONE scratch per device, shared by every context: two calls
+ *    whose launches overlap (different streams, threads or contexts without
+ *    ordering between them) race on it and give wrong results.  Order them
+ *    on one stream or synchronise between them. */
+#define DGSEM_STATIC_SCRATCH_MAX_STATE 2097152
+dgsem_status dgsem_ssprk3_step_static_scratch(dgsem_ctx* ctx, double* u,
+                                              double t, double dt);
 
 /* nsteps SSPRK3 steps on a HOST array (the reference's host-side view of
  * the state): copies u_host to the device, steps, copies back and
