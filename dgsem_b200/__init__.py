@@ -14,4 +14,4 @@ from .solver import (  # noqa: F401
     SSPRK3, StructuredMesh, StructuredSolver, TaylorGreenVortex2D,
     VolumeIntegralShockCapturingHG, VolumeIntegralSplitForm,
 )
-from .solver import BatchGraph, BatchSolver  # noqa: F401,E402
+from .solver import Adjoint, BatchGraph, BatchSolver  # noqa: F401,E402

@@ -17,30 +17,11 @@
 #include <vector>
 
 #include "../../include/dgsem_b200.h"
+#include "context.hpp"
 #include "engine.cuh"
 #include "tables.hpp"
 
 using namespace dgsem;
-
-struct dgsem_ctx {
-  dgsem_mesh_desc mesh;
-  dgsem_scheme_desc scheme;
-  cudaStream_t stream = nullptr;
-  int device = 0;
-  EngineConfig cfg{};
-  std::unique_ptr<EngineBase> engine;
-  int nodes = 0;     // n^d
-  int nvars = 0;
-  int64_t state_len = 0;
-  std::vector<void*> allocations;
-  double* tmp1 = nullptr;  // SSPRK3 stage states
-  double* tmp2 = nullptr;
-  double* staging = nullptr;  // device copy for the host-buffer entry point
-  double* tdev = nullptr;     // device clock for graph replay
-  double* table_block = nullptr;
-  unsigned int* flag = nullptr;
-  int64_t launches = 0;
-};
 
 namespace {
 

@@ -52,8 +52,8 @@ extern "C" dgsem_status dgsem_ssprk3_step_static_scratch(dgsem_ctx* ctx, double*
                                                          double dt) {
   if (!ctx || !u) return DGSEM_ERR_INVALID_ARG;
   int64_t nelem = 0, state_len = 0;
-  int nvars = 0, nodes = 0;
-  dgsem_status st = dgsem_get_sizes(ctx, &nelem, &nvars, &nodes, &state_len);
+  int nodes = 0, nvars = 0;
+  dgsem_status st = dgsem_get_sizes(ctx, &nelem, &nodes, &nvars, &state_len);
   if (st != DGSEM_OK) return st;
   if (state_len > DGSEM_STATIC_SCRATCH_MAX_STATE) return DGSEM_ERR_SCRATCH_LIMIT;
   // The scratch address is per device: u must live on the current device.

@@ -404,6 +404,54 @@ class SSPRK3:
                 break
 
 
+# ---------------------------------------------------------------- discrete adjoint
+class Adjoint:
+    """Discrete adjoint of a StructuredSolver's right-hand side and of SSPRK3
+    (dgsem_adjoint_* in include/dgsem_b200.h): 2D periodic meshes, the
+    Chandrashekar split form with the LLF surface flux, Euler or
+    Navier-Stokes.  `nsteps` SSPRK3 steps with a checkpoint every
+    `checkpoint_every` steps."""
+
+    def __init__(self, solver: StructuredSolver, nsteps: int, checkpoint_every: int = 20):
+        self.solver = solver
+        self.nsteps, self.checkpoint_every = int(nsteps), int(checkpoint_every)
+        h = ctypes.c_void_p()
+        C.check(C.lib().dgsem_adjoint_create(solver.handle, self.nsteps, self.checkpoint_every,
+                                             ctypes.byref(h)), "dgsem_adjoint_create")
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            C.lib().dgsem_adjoint_destroy(h)
+            self._h = None
+
+    def rhs_vjp(self, u: torch.Tensor, w: torch.Tensor) -> torch.Tensor:
+        """(dR/du(u))^T w."""
+        out = torch.empty_like(w)
+        C.check(C.lib().dgsem_adjoint_rhs_vjp(self._h, _ptr(u), _ptr(w), _ptr(out)),
+                "dgsem_adjoint_rhs_vjp")
+        return out
+
+    def kinetic_energy(self, u: torch.Tensor, grad: bool = False):
+        """Mean kinetic energy J(u) (and dJ/du when grad is True)."""
+        val = ctypes.c_double()
+        g = torch.empty_like(u) if grad else None
+        C.check(C.lib().dgsem_kinetic_energy(self._h, _ptr(u), ctypes.byref(val),
+                                             _ptr(g) if grad else None),
+                "dgsem_kinetic_energy")
+        return (val.value, g) if grad else val.value
+
+    def gradient(self, u0: torch.Tensor, t0: float, dt: float):
+        """J(u(t0 + nsteps dt)) and dJ/du0 (all variables; u0 is not modified)."""
+        val = ctypes.c_double()
+        g = torch.empty_like(u0)
+        C.check(C.lib().dgsem_adjoint_gradient(self._h, _ptr(u0), float(t0), float(dt),
+                                               ctypes.byref(val), _ptr(g)),
+                "dgsem_adjoint_gradient")
+        return val.value, g
+
+
 # ---------------------------------------------------------------- batched mode
 class BatchSolver:
     """Many independent periodic meshes (uneven sizes and degrees) sharing one

@@ -282,6 +282,43 @@ dgsem_status dgsem_set_launch_variant(dgsem_ctx* ctx, int variant);
 /* Number of kernel launches issued by this context so far (diagnostics). */
 dgsem_status dgsem_launch_count(const dgsem_ctx* ctx, int64_t* count);
 
+/* ---------------------------------------------------------------------------
+ * Discrete adjoint (no reference counterpart): transposed linearisation of
+ * the forward kernels' arithmetic and of SSPRK3, for 2D periodic meshes with
+ * the Chandrashekar split form, LLF surface flux, Euler or Navier-Stokes
+ * (BR1).  Other schemes return DGSEM_ERR_UNSUPPORTED.
+ * ------------------------------------------------------------------------- */
+typedef struct dgsem_adjoint dgsem_adjoint;
+
+/* Workspace for nsteps SSPRK3 steps with a checkpoint every checkpoint_every
+ * steps: ceil(nsteps / every) saved states plus 3 * every stage states of
+ * one segment, all in device memory. */
+dgsem_status dgsem_adjoint_create(dgsem_ctx* ctx, int nsteps, int checkpoint_every,
+                                  dgsem_adjoint** out);
+dgsem_status dgsem_adjoint_destroy(dgsem_adjoint* adj);
+
+/* out = (dR/du(u))^T w, with R the right-hand side of dgsem_rhs.  out must
+ * not alias w. */
+dgsem_status dgsem_adjoint_rhs_vjp(dgsem_adjoint* adj, const double* u,
+                                   const double* w, double* out);
+
+/* Volume-weighted mean kinetic energy J(u) = sum w |m|^2/(2 rho) / sum w
+ * with w = w_i w_j / |1/J| (analyzer/volume_average_euler.hpp:9-69) to the
+ * host (value, may be NULL; synchronises when given) and dJ/du to the device
+ * array grad (may be NULL). */
+dgsem_status dgsem_kinetic_energy(dgsem_adjoint* adj, const double* u,
+                                  double* value, double* grad);
+
+/* Gradient of J(u(t0 + nsteps dt)) with respect to the initial state u0:
+ * forward SSPRK3 with checkpoints, then the reverse sweep (each segment's
+ * stage states recomputed from its checkpoint, the last one recorded during
+ * the forward pass).  u0 is not modified; *value receives J (may be NULL);
+ * grad_u0 (device, state layout) receives dJ/du0 for every variable.
+ * Synchronous. */
+dgsem_status dgsem_adjoint_gradient(dgsem_adjoint* adj, const double* u0,
+                                    double t0, double dt, double* value,
+                                    double* grad_u0);
+
 /* Host-side copies of the basis tables (nodes, weights, inv_weights,
  * lhat(-1), lhat(+1), D, Dsplit, Dhat, inverse Legendre Vandermonde; the
  * n x n tables row-major) for polydeg N; out needs 5n + 4n^2 doubles.

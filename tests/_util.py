@@ -54,3 +54,36 @@ CASES = {
     "ns": dict(ndims=2, polydeg=4, cells=(6, 6), left=(0.0, 0.0), right=(2 * math.pi,) * 2,
                ic="tgv2d", viscous=True, mu=1.0e-3, prandtl=0.72, noise=1.0e-3),
 }
+
+
+# The adjoint workload: 2D Navier-Stokes Taylor-Green vortex on [0, 2 pi]^2,
+# 32 x 32 elements, N = 4, Re = 1000 (mu = 1e-3), Pr = 0.72, plus 1e-3
+# seeded Gaussian noise on the momentum; 200 SSPRK3 steps of dt = 1e-3
+# (CFL ~0.5 for lambda_max ~11 with the reference's dt rule), checkpoints
+# every 20 steps; objective = mean kinetic energy of the final state.
+ADJOINT_CASE = dict(ndims=2, polydeg=4, cells=(32, 32), left=(0.0, 0.0),
+                    right=(2 * math.pi, 2 * math.pi), viscous=True, mu=1.0e-3, prandtl=0.72)
+ADJOINT_NOISE, ADJOINT_SEED = 1.0e-3, 0
+ADJOINT_STEPS, ADJOINT_DT, ADJOINT_EVERY = 200, 1.0e-3, 20
+ADJOINT_DIRECTION_SEED, ADJOINT_DIRECTIONS = 2024, 8
+
+
+def adjoint_initial_state():
+    """(oracle scheme, u0 in the reference layout u(i, j, dof, var))."""
+    from oracle import dgsem_oracle as do
+    s = do.Scheme(**ADJOINT_CASE)
+    u = do.initial_state(s, "tgv2d")
+    rng = np.random.default_rng(ADJOINT_SEED)
+    u[..., 1:3] += ADJOINT_NOISE * rng.standard_normal(u[..., 1:3].shape)
+    return s, np.ascontiguousarray(u)
+
+
+def adjoint_directions(u0: np.ndarray):
+    """Seeded Gaussian directions in the initial momentum (reference layout)."""
+    rng = np.random.default_rng(ADJOINT_DIRECTION_SEED)
+    out = []
+    for _ in range(ADJOINT_DIRECTIONS):
+        d = np.zeros_like(u0)
+        d[..., 1:3] = rng.standard_normal(u0[..., 1:3].shape)
+        out.append(d)
+    return out

@@ -162,3 +162,34 @@ def test_free_stream_preservation_3d():
     u = np.zeros(s.geo.inv_j.shape + (5,))
     u[..., :] = do.prim_to_cons([1.0, 0.3, -0.2, 0.1, 71.4], 1.4)
     assert np.max(np.abs(do.rhs(s, u))) <= 1e-9
+
+
+# ---- tangent-linear reference (dual-number build of the reference) ---------
+from oracle import ref_tlm_binding as tb  # noqa: E402
+
+
+@pytest.mark.skipif(not (tb.available() and rb.available()),
+                    reason="compiled reference (oracle/_ref) not built")
+@pytest.mark.parametrize("name", ["kh", "ns"])
+def test_tangent_linear_reference_value_and_tangent(name):
+    """The dual-number build returns the double build's RHS bit for bit, and
+    its tangent matches central differences of the reference RHS at a step
+    small enough not to cross the LLF max()/abs() kinks."""
+    g = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    c = CASE_SCHEMES[name]
+    kind = tb.NS2D if c.get("viscous") else tb.EULER2D
+    tc = tb.TangentCase(kind, c["polydeg"], c["cells"], c["left"], c["right"], 1.4,
+                        c.get("mu", 0.0), c.get("prandtl", 0.72))
+    ref = rb.RefCase(kind=rb.NS2D_PERIODIC_SPLIT if c.get("viscous") else
+                     rb.EULER2D_PERIODIC_SPLIT, polydeg=c["polydeg"], n_cells=c["cells"],
+                     left=c["left"], right=c["right"], mu=c.get("mu", 0.0),
+                     prandtl=c.get("prandtl", 0.72))
+    u = np.ascontiguousarray(g["u"])
+    t = float(g["t"])
+    rng = np.random.default_rng(5)
+    d = rng.standard_normal(u.shape)
+    r, dr = tc.rhs(u, d, t)
+    assert np.array_equal(r, ref.rhs(u, t))
+    h = 1.0e-9
+    fd = (ref.rhs(u + h * d, t) - ref.rhs(u - h * d, t)) / (2.0 * h)
+    assert np.max(np.abs(fd - dr)) <= 1e-5 * np.max(np.abs(dr))
