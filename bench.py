@@ -536,13 +536,130 @@ def run_batched(args):
     return 0
 
 
+def run_adjoint(args):
+    """Adjoint workload: gradient of the final mean kinetic energy of a 2D
+    Navier-Stokes Taylor-Green vortex (32 x 32 elements, N = 4, Re = 1000,
+    Pr = 0.72, 1e-3 seeded momentum noise) after 200 SSPRK3 steps of
+    dt = 1e-3, with respect to the initial state; checkpoints every 20 steps.
+    Reports the cost of the gradient relative to the forward run."""
+    import ctypes
+
+    import torch
+
+    import dgsem_b200 as D
+    from dgsem_b200 import _capi as C
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    nsteps, every, dt, cells, N = 200, 20, 1.0e-3, (32, 32), 4
+    mesh = D.StructuredMesh((0.0, 0.0), (2 * math.pi, 2 * math.pi), cells)
+    basis = D.LobattoLegendreBasis(N)
+    eq = D.CompressibleNavierStokes2D(1.4, 1.0e-3, 0.72)
+    solver = D.StructuredSolver(eq, basis, D.VolumeIntegralSplitForm(D.ChandrashekarFlux),
+                                D.LaxFriedrichsFlux(), mesh,
+                                D.BoundarySet(*[D.PeriodicBC() for _ in range(4)]))
+    sol = D.Solution(mesh, basis, eq, device=dev)
+    solver.initialize(D.TaylorGreenVortex2D(), sol)
+    gen = torch.Generator(device=dev).manual_seed(0)
+    sol.u[:, 1:3, :] += 1.0e-3 * torch.randn(sol.u[:, 1:3, :].shape, generator=gen,
+                                             device=dev, dtype=torch.float64)
+    u0 = sol.u.clone()
+    dofs = math.prod(cells) * (N + 1) ** 2
+    adj = D.Adjoint(solver, nsteps, every)
+    stream = solver.stream
+    L = C.lib()
+    work = u0.clone()
+
+    def forward():
+        work.copy_(u0)
+        C.check(L.dgsem_ssprk3_steps(solver.handle, ctypes.c_void_p(work.data_ptr()), 0.0, dt,
+                                     nsteps), "dgsem_ssprk3_steps")
+
+    reps = max(1, min(args.steps, 5))
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            forward()
+            adj.gradient(u0, 0.0, dt)
+        torch.cuda.synchronize()
+        sampler = ClockSampler(dev.index)
+        sampler.start()
+        fwd, grad_ms = [], []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            forward()
+            b.record(stream)
+            torch.cuda.synchronize()
+            fwd.append(a.elapsed_time(b))
+        launches0 = solver.launch_count()
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            J, g = adj.gradient(u0, 0.0, dt)
+            b.record(stream)
+            torch.cuda.synchronize()
+            grad_ms.append(a.elapsed_time(b))
+        launches = (solver.launch_count() - launches0) // reps
+        clocks = sampler.stop()
+        # e2e: initial state from pinned host memory, gradient back to host
+        host_u0 = u0.detach().to("cpu").pin_memory()
+        host_g = torch.empty_like(host_u0).pin_memory()
+        dev_u0 = torch.empty_like(u0)
+        e2e = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            dev_u0.copy_(host_u0, non_blocking=True)
+            _, gg = adj.gradient(dev_u0, 0.0, dt)
+            host_g.copy_(gg, non_blocking=True)
+            torch.cuda.synchronize()
+            e2e.append((time.perf_counter() - t0) * 1e3)
+        # one seeded central-difference check of the gradient
+        d = torch.zeros_like(u0)
+        d[:, 1:3, :] = torch.randn(d[:, 1:3, :].shape, generator=gen, device=dev,
+                                   dtype=torch.float64)
+        eps = 1.0e-6
+
+        def J_of(v):
+            w = v.clone()
+            C.check(L.dgsem_ssprk3_steps(solver.handle, ctypes.c_void_p(w.data_ptr()), 0.0, dt,
+                                         nsteps), "dgsem_ssprk3_steps")
+            return adj.kinetic_energy(w)
+
+        fd = (J_of(u0 + eps * d) - J_of(u0 - eps * d)) / (2 * eps)
+        ad = float(torch.sum(g * d))
+    fwd_ms, adj_ms = statistics.median(fwd), statistics.median(grad_ms)
+    line = {
+        "metric": "adjoint gradient cost / forward cost", "value": adj_ms / fwd_ms,
+        "unit": "x forward", "n_gpus": 1, "steps": reps, "warmup": args.warmup,
+        "ms_per_step": adj_ms / nsteps, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (Taylor-Green vortex + seeded Gaussian momentum noise)",
+        "config": {"workload": "adjoint", "equation": "navier_stokes2d", "mesh": list(cells),
+                   "polydeg": N, "dofs": dofs, "mu": 1.0e-3, "prandtl": 0.72,
+                   "ssprk3_steps": nsteps, "dt": dt, "checkpoint_every": every,
+                   "objective": "mean kinetic energy of the final state",
+                   "volume_flux": "chandrashekar", "surface_flux": "llf",
+                   "l2": "state 0.8 MB is L2-resident (launch-latency bound workload)"},
+        "forward_ms": fwd_ms, "adjoint_gradient_ms": adj_ms,
+        "reverse_only_ratio": (adj_ms - fwd_ms) / fwd_ms,
+        "objective": J,
+        "fd_check": {"eps": eps, "fd": fd, "adjoint": ad, "rel": abs(fd - ad) / abs(ad)},
+        "e2e": {"value": statistics.median(e2e) / fwd_ms, "unit": "x forward",
+                "ms": statistics.median(e2e), "h2d_bytes_per_step": u0.numel() * 8,
+                "d2h_bytes_per_step": u0.numel() * 8},
+        "gpu_launches": launches, "clocks": clocks,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="dgsem_b200", choices=["dgsem_b200", "reference"])
-    ap.add_argument("--workload", default="tgv16", choices=list(WORKLOADS) + ["batched"])
+    ap.add_argument("--workload", default="tgv16",
+                    choices=list(WORKLOADS) + ["batched", "adjoint"])
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variant", default="auto", choices=["auto", "0", "1", "2"],
@@ -556,6 +673,12 @@ def main():
                               "the reference has no batched multi-mesh mode"}))
             return 0
         return run_batched(args)
+    if args.workload == "adjoint":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the reference has no adjoint"}))
+            return 0
+        return run_adjoint(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_device_arm(args)
