@@ -44,7 +44,7 @@ EXPORTED = [
     "dgsem_batch_launch_count", "dgsem_autotune", "dgsem_set_launch_variant",
     "dgsem_batch_autotune", "dgsem_ssprk3_step_static_scratch",
     "dgsem_adjoint_create", "dgsem_adjoint_destroy", "dgsem_adjoint_rhs_vjp",
-    "dgsem_kinetic_energy", "dgsem_adjoint_gradient",
+    "dgsem_kinetic_energy", "dgsem_adjoint_gradient", "dgsem_coordinates_host",
 ]
 
 
@@ -104,6 +104,7 @@ def lib() -> ctypes.CDLL:
     L.dgsem_basis_tables_host.argtypes = [c.c_int, c.POINTER(c.c_double)]
     L.dgsem_metrics_host.argtypes = [c.POINTER(MeshDesc), c.POINTER(c.c_double),
                                      c.POINTER(c.c_double)]
+    L.dgsem_coordinates_host.argtypes = [c.POINTER(MeshDesc), c.POINTER(c.c_double)]
     L.dgsem_ssprk3_steps_host.argtypes = [vp, vp, c.c_double, c.c_double, c.c_int]
     L.dgsem_graph_create.argtypes = [vp, dp, c.c_double, c.c_int, c.POINTER(vp)]
     L.dgsem_graph_launch.argtypes = [vp, c.c_double]

@@ -820,4 +820,31 @@ dgsem_status dgsem_metrics_host(const dgsem_mesh_desc* mesh, double* ja,
   return DGSEM_OK;
 }
 
+dgsem_status dgsem_coordinates_host(const dgsem_mesh_desc* mesh, double* coords) {
+  if (!mesh || !coords || (mesh->ndims != 2 && mesh->ndims != 3)) return DGSEM_ERR_INVALID_ARG;
+  BasisTables b;
+  if (!make_basis(mesh->polydeg, &b)) return DGSEM_ERR_INVALID_ARG;
+  MetricTablesHost mt;
+  int64_t cells[3] = {1, 1, 1};
+  for (int a = 0; a < mesh->ndims; ++a) cells[a] = mesh->n_cells[a];
+  if (!make_metric_tables(b, mesh->ndims, cells, mesh->domain_left, mesh->domain_right, &mt))
+    return DGSEM_ERR_INVALID_ARG;
+  const int nd = mesh->ndims;
+  const int n = b.n;
+  const int ND = nd == 2 ? n * n : n * n * n;
+  // reference logical order: cells (i slowest) x dof x dim
+  for (int64_t ie = 0; ie < cells[0]; ++ie)
+    for (int64_t je = 0; je < cells[1]; ++je)
+      for (int64_t ke = 0; ke < cells[2]; ++ke) {
+        const int64_t eref = nd == 2 ? ie * cells[1] + je : (ie * cells[1] + je) * cells[2] + ke;
+        const int64_t ev[3] = {ie, je, ke};
+        for (int node = 0; node < ND; ++node) {
+          const int iv[3] = {node % n, (node / n) % n, node / (n * n)};
+          for (int a = 0; a < nd; ++a)
+            coords[(eref * ND + node) * nd + a] = mt.coord[a][ev[a] * n + iv[a]];
+        }
+      }
+  return DGSEM_OK;
+}
+
 }  // extern "C"

@@ -18,7 +18,7 @@
  * (LaxFriedrichsFlux + 2D HLLC), volume integral (VolumeIntegralSplitForm /
  * VolumeIntegralShockCapturingHG) and one boundary condition per mesh face
  * (BoundarySet of PeriodicBC, DirichletBC, OutflowBC,
- * MixedDirichletSlipWallBC; src/boundary_condition/*.hpp).
+ * MixedDirichletSlipWallBC; src/boundary_condition/ headers).
  *
  * Data layout on the device (all FP64, caller-owned):
  *   state u[e][var][node], e = ie + nx*(je + ny*ke), node = in + n*(jn + n*kn)
@@ -330,6 +330,11 @@ dgsem_status dgsem_basis_tables_host(int polydeg, double* out);
  * ja(cells..., dof, a, c), inv_j(cells..., dof).  No GPU needed. */
 dgsem_status dgsem_metrics_host(const dgsem_mesh_desc* mesh, double* ja,
                                 double* inv_j);
+
+/* Host-side node coordinates of the mesh's LinearMapping (the reference's
+ * container.node_coordinates, data_container.hpp:729-772) in the logical
+ * layout coords(cells..., dof, dim).  No GPU needed. */
+dgsem_status dgsem_coordinates_host(const dgsem_mesh_desc* mesh, double* coords);
 
 #ifdef __cplusplus
 }
