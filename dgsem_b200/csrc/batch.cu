@@ -30,6 +30,7 @@ struct Group {
   EngineConfig cfg{};
   std::vector<int> members;       // mesh indices of this degree
   int ntiles = 0;
+  size_t tile_capacity = 0;       // entries of tile_mesh / tile_e0
   int* tile_mesh = nullptr;       // device
   int* tile_e0 = nullptr;         // device
   cudaStream_t stream = nullptr;  // fork stream
@@ -158,6 +159,7 @@ cudaError_t build_tiles(const dgsem_batch* b, Group& g) {
       tm.push_back(m);
       te.push_back((int)e0);
     }
+  if (tm.size() > g.tile_capacity) return cudaErrorInvalidValue;
   g.ntiles = (int)tm.size();
   cudaError_t e = cudaMemcpy(g.tile_mesh, tm.data(), tm.size() * sizeof(int),
                              cudaMemcpyHostToDevice);
@@ -182,7 +184,7 @@ dgsem_status dgsem_batch_autotune(dgsem_batch* b, double* u, const double* dt_ho
   for (Group& g : b->groups) {
     int best = 0;
     float best_ms = 1e30f;
-    for (int v = 0; v < kNumVariants && st == DGSEM_OK; ++v) {
+    for (int v = 0; v < g.engine->num_variants() && st == DGSEM_OK; ++v) {
       g.engine->set_variant(v);
       if (build_tiles(b, g) != cudaSuccess) st = DGSEM_ERR_CUDA;
       // stage 1 writes tmp1 only, so repeated launches leave u untouched
@@ -331,12 +333,11 @@ dgsem_status dgsem_batch_create(const dgsem_mesh_desc* meshes, int n_meshes,
     c.grad = nullptr;
     for (int f = 0; f < 6; ++f) c.bc.kind[f] = 0;
     g.members = kv.second;
-    // tile arrays sized for the smallest elements-per-block shape
+    // tile arrays sized for one element per tile (any launch shape fits)
     g.engine->set_variant(0);
     size_t max_tiles = 0;
-    for (int m : g.members)
-      max_tiles += (b->nelem[m] + g.engine->elements_per_block() - 1) /
-                   g.engine->elements_per_block();
+    for (int m : g.members) max_tiles += (size_t)b->nelem[m];
+    g.tile_capacity = max_tiles;
     g.tile_mesh = balloc<int>(b, max_tiles);
     g.tile_e0 = balloc<int>(b, max_tiles);
     if (!g.tile_mesh || !g.tile_e0) {

@@ -696,6 +696,10 @@ int time_variants(EngineBase* eng, cudaStream_t s, Launch&& launch, double* time
   int best = 0;
   float best_ms = 1e30f;
   for (int v = 0; v < kNumVariants; ++v) {
+    if (v >= eng->num_variants()) {
+      if (times_ms) times_ms[v] = 0.0;
+      continue;
+    }
     eng->set_variant(v);
     launch();  // warm-up
     cudaEventRecord(a, s);
@@ -722,7 +726,7 @@ int time_variants(EngineBase* eng, cudaStream_t s, Launch&& launch, double* time
 extern "C" {
 
 dgsem_status dgsem_set_launch_variant(dgsem_ctx* ctx, int variant) {
-  if (!ctx || variant < 0 || variant >= kNumVariants) return DGSEM_ERR_INVALID_ARG;
+  if (!ctx || variant < 0 || variant >= ctx->engine->num_variants()) return DGSEM_ERR_INVALID_ARG;
   ctx->engine->set_variant(variant);
   return DGSEM_OK;
 }

@@ -13,6 +13,7 @@
 
 #include "br1_kernel.cuh"
 #include "stage_kernel.cuh"
+#include "stage_node_kernel.cuh"
 #include "tables.hpp"
 
 namespace dgsem {
@@ -35,7 +36,10 @@ struct EngineConfig {
   double* grad;             // Navier-Stokes lifted gradient [E][4][2][n^2]
 };
 
-constexpr int kNumVariants = 3;
+// Launch-shape variants: 0-2 line-parallel (stage_kernel.cuh), 3
+// node-parallel (stage_node_kernel.cuh; split form without shock capturing
+// or viscous terms only).
+constexpr int kNumVariants = 4;
 
 class EngineBase {
  public:
@@ -56,9 +60,10 @@ class EngineBase {
   virtual int elements_per_block() const = 0;
   virtual int threads_per_block() const = 0;
   virtual size_t smem_bytes() const = 0;
-  // launch-shape variant in [0, kNumVariants)
+  // launch-shape variant in [0, num_variants())
   virtual void set_variant(int v) = 0;
   virtual int variant() const = 0;
+  virtual int num_variants() const = 0;
 };
 
 std::unique_ptr<EngineBase> make_engine(int ndims, int n, int vf, int sf,
@@ -99,6 +104,14 @@ struct LaunchShape {
   static constexpr int MINB = V == 1 ? (65536 / (NT * 100) > 1 ? 65536 / (NT * 100) : 2) : 0;
 };
 
+// Node-parallel variant: about 128 threads per block, one per node.
+template <int DIM, int N>
+struct NodeLaunch {
+  static constexpr int ND = ipow(N, DIM);
+  static constexpr int EPB = (128 / ND) > 0 ? (128 / ND) : 1;
+  static constexpr int NT = EPB * ND;
+};
+
 template <int DIM, int N, int VF, int SF, bool HG, bool NS = false>
 class Engine final : public EngineBase {
  public:
@@ -134,10 +147,23 @@ class Engine final : public EngineBase {
                            (int)Sh<V>::smem_bytes);
   }
 
+  using NL = NodeLaunch<DIM, N>;
+  using NSh = NodeShape<DIM, N, VF, NL::EPB>;
+  template <bool B>
+  static auto node_kernel() {
+    return stage_node_kernel<DIM, N, VF, SF, NL::EPB, B>;
+  }
+
   Engine() {
     set_attributes<0>();
     set_attributes<1>();
     set_attributes<2>();
+    if constexpr (kBatch) {
+      cudaFuncSetAttribute(node_kernel<false>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)NSh::smem_bytes);
+      cudaFuncSetAttribute(node_kernel<true>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)NSh::smem_bytes);
+    }
   }
 
   StageArgs<N> common_args(const EngineConfig& cfg, double a, double b, double t,
@@ -202,6 +228,12 @@ class Engine final : public EngineBase {
     switch (variant_) {
       case 1: launch<1>(args, cfg.nelem, s); break;
       case 2: launch<2>(args, cfg.nelem, s); break;
+      case 3:
+        if constexpr (kBatch) {
+          const int64_t blocks = (cfg.nelem + NL::EPB - 1) / NL::EPB;
+          node_kernel<false>()<<<(unsigned)blocks, NL::NT, NSh::smem_bytes, s>>>(args);
+        }
+        break;
       default: launch<0>(args, cfg.nelem, s); break;
     }
     return cudaGetLastError();
@@ -229,6 +261,7 @@ class Engine final : public EngineBase {
       switch (variant_) {
         case 1: launch_batch<1>(args, ntiles, s); break;
         case 2: launch_batch<2>(args, ntiles, s); break;
+        case 3: node_kernel<true>()<<<(unsigned)ntiles, NL::NT, NSh::smem_bytes, s>>>(args); break;
         default: launch_batch<0>(args, ntiles, s); break;
       }
       return cudaGetLastError();
@@ -237,16 +270,20 @@ class Engine final : public EngineBase {
 
   int kernels_per_stage() const override { return NS ? 2 : 1; }
   int elements_per_block() const override {
+    if (variant_ == 3) return NL::EPB;
     return variant_ == 2 ? LaunchShape<DIM, N, 2>::EPB : LaunchShape<DIM, N, 0>::EPB;
   }
   int threads_per_block() const override {
+    if (variant_ == 3) return NL::NT;
     return variant_ == 2 ? LaunchShape<DIM, N, 2>::NT : LaunchShape<DIM, N, 0>::NT;
   }
   size_t smem_bytes() const override {
+    if (variant_ == 3) return NSh::smem_bytes;
     return variant_ == 2 ? Sh<2>::smem_bytes : Sh<0>::smem_bytes;
   }
-  void set_variant(int v) override { variant_ = (v >= 0 && v < kNumVariants) ? v : 0; }
+  void set_variant(int v) override { variant_ = (v >= 0 && v < num_variants()) ? v : 0; }
   int variant() const override { return variant_; }
+  int num_variants() const override { return kBatch ? 4 : 3; }
 
  private:
   int variant_ = 0;

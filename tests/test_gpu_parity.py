@@ -290,10 +290,11 @@ def test_conservation_and_free_stream_large(cuda):
     assert float(du.abs().max()) <= 1e-10 * float(fs.abs().max()) / h
 
 
-@pytest.mark.parametrize("name", ["kh", "kh_hg", "dmr", "tgv", "ns"])
-def test_launch_variants_bitwise_identical(name, cuda):
-    """Every launch shape of the fused stage kernel gives the same bits, and
-    the autotuner leaves the state untouched and keeps a valid shape."""
+@pytest.mark.parametrize("name", ["kh", "kh_hg", "dmr", "tgv", "ns", "vortex_n6"])
+def test_launch_variants(name, cuda):
+    """The line-parallel launch shapes give the same bits, the node-parallel
+    shape agrees to rounding and with the oracle, and the autotuner leaves
+    the state untouched and keeps a valid shape."""
     import torch
     case = CASES[name]
     s = make_oracle(case)
@@ -311,12 +312,58 @@ def test_launch_variants_bitwise_identical(name, cuda):
     torch.cuda.synchronize()
     for v in (1, 2):
         assert torch.equal(outs[0], outs[v]), v
+    node_variant = not (case.get("shock_capturing") or case.get("viscous"))
+    if node_variant:
+        # node-parallel shape: same arithmetic per flux, different summation
+        # order (each pair evaluated by both of its nodes)
+        solver.set_launch_variant(3)
+        du3 = torch.empty_like(u)
+        solver.rhs(u, du3, 0.05)
+        torch.cuda.synchronize()
+        a, b = du3.cpu().numpy(), outs[0].cpu().numpy()
+        assert rel_linf(a, b) <= RTOL
+        assert rel_linf(dev_to_ref(a, solver.mesh.n_cells), do.rhs(s, u_ref, 0.05)) <= RTOL
+    else:
+        with pytest.raises(Exception):
+            solver.set_launch_variant(3)
     chosen, times = solver.autotune(u, retime=True)
     torch.cuda.synchronize()
-    assert chosen in (0, 1, 2)
-    assert all(t > 0.0 for t in times)
+    assert chosen in ((0, 1, 2, 3) if node_variant else (0, 1, 2))
+    assert all(t > 0.0 for t in times[:4 if node_variant else 3])
     assert torch.equal(u, u_copy)
     du = torch.empty_like(u)
     solver.rhs(u, du, 0.05)
     torch.cuda.synchronize()
-    assert torch.equal(du, outs[0])
+    if chosen < 3:
+        assert torch.equal(du, outs[0])
+
+
+@pytest.mark.parametrize("vf", ["chandrashekar", "ranocha", "kennedy_gruber"])
+@pytest.mark.parametrize("sf", ["llf", "hllc"])
+def test_node_parallel_variant_other_fluxes(vf, sf, cuda):
+    """The node-parallel launch shape with every two-point / surface flux
+    (plain split form) against the oracle, 2D KH and (LLF) 3D TGV."""
+    for name in (["kh", "tgv"] if sf == "llf" else ["kh"]):
+        case = CASES[name]
+        s = make_oracle(case, vf, sf)
+        u = initial(case, s, seed=3)
+        du_o = do.rhs(s, u, 0.0)
+        solver = make_device(case, vf, sf)
+        solver.set_launch_variant(3)
+        du_d = device_rhs(solver, u, 0.0, cuda)
+        assert rel_linf(du_d, du_o) <= RTOL, (name, rel_linf(du_d, du_o))
+
+
+def test_node_parallel_variant_dmr_boundaries(cuda):
+    """Node-parallel shape with the DMR boundary conditions (no shock
+    capturing: the same BC code path as the line-parallel shapes)."""
+    case = dict(CASES["dmr"])
+    case.pop("shock_capturing")
+    s = make_oracle(case, "chandrashekar", "llf")
+    u = initial(case, s)
+    t = 0.02
+    du_o = do.rhs(s, u, t)
+    solver = make_device(case)
+    solver.set_launch_variant(3)
+    du_d = device_rhs(solver, u, t, cuda)
+    assert rel_linf(du_d, du_o) <= RTOL, rel_linf(du_d, du_o)
