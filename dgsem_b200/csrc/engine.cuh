@@ -36,10 +36,10 @@ struct EngineConfig {
   double* grad;             // Navier-Stokes lifted gradient [E][4][2][n^2]
 };
 
-// Launch-shape variants: 0-2 line-parallel (stage_kernel.cuh), 3
+// Launch-shape variants: 0-2 line-parallel (stage_kernel.cuh), 3-4
 // node-parallel (stage_node_kernel.cuh; split form without shock capturing
 // or viscous terms only).
-constexpr int kNumVariants = 4;
+constexpr int kNumVariants = 5;
 
 class EngineBase {
  public:
@@ -104,12 +104,15 @@ struct LaunchShape {
   static constexpr int MINB = V == 1 ? (65536 / (NT * 100) > 1 ? 65536 / (NT * 100) : 2) : 0;
 };
 
-// Node-parallel variant: about 128 threads per block, one per node.
+// Node-parallel variants: about 128 threads per block, one per node;
+// variant 3 caps registers at ~72 per thread (7 resident blocks of 128),
+// variant 4 leaves them to the compiler.
 template <int DIM, int N>
 struct NodeLaunch {
   static constexpr int ND = ipow(N, DIM);
   static constexpr int EPB = (128 / ND) > 0 ? (128 / ND) : 1;
   static constexpr int NT = EPB * ND;
+  static constexpr int MINB = 65536 / (NT * 72) > 1 ? 65536 / (NT * 72) : 1;
 };
 
 template <int DIM, int N, int VF, int SF, bool HG, bool NS = false>
@@ -149,9 +152,24 @@ class Engine final : public EngineBase {
 
   using NL = NodeLaunch<DIM, N>;
   using NSh = NodeShape<DIM, N, VF, NL::EPB>;
-  template <bool B>
+  template <bool B, bool CAP>
   static auto node_kernel() {
-    return stage_node_kernel<DIM, N, VF, SF, NL::EPB, B>;
+    if constexpr (CAP)
+      return stage_node_kernel_capped<DIM, N, VF, SF, NL::EPB, B, NL::MINB>;
+    else
+      return stage_node_kernel<DIM, N, VF, SF, NL::EPB, B>;
+  }
+  template <bool CAP>
+  void launch_node(const StageArgs<N>& args, int64_t nelem, cudaStream_t s) const {
+    if constexpr (kBatch) {
+      const int64_t blocks = (nelem + NL::EPB - 1) / NL::EPB;
+      node_kernel<false, CAP>()<<<(unsigned)blocks, NL::NT, NSh::smem_bytes, s>>>(args);
+    }
+  }
+  template <bool CAP>
+  void launch_node_batch(const StageArgs<N>& args, int ntiles, cudaStream_t s) const {
+    if constexpr (kBatch)
+      node_kernel<true, CAP>()<<<(unsigned)ntiles, NL::NT, NSh::smem_bytes, s>>>(args);
   }
 
   Engine() {
@@ -159,10 +177,11 @@ class Engine final : public EngineBase {
     set_attributes<1>();
     set_attributes<2>();
     if constexpr (kBatch) {
-      cudaFuncSetAttribute(node_kernel<false>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)NSh::smem_bytes);
-      cudaFuncSetAttribute(node_kernel<true>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)NSh::smem_bytes);
+      const int sm = (int)NSh::smem_bytes;
+      cudaFuncSetAttribute(node_kernel<false, true>(), cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+      cudaFuncSetAttribute(node_kernel<true, true>(), cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+      cudaFuncSetAttribute(node_kernel<false, false>(), cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+      cudaFuncSetAttribute(node_kernel<true, false>(), cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     }
   }
 
@@ -228,12 +247,8 @@ class Engine final : public EngineBase {
     switch (variant_) {
       case 1: launch<1>(args, cfg.nelem, s); break;
       case 2: launch<2>(args, cfg.nelem, s); break;
-      case 3:
-        if constexpr (kBatch) {
-          const int64_t blocks = (cfg.nelem + NL::EPB - 1) / NL::EPB;
-          node_kernel<false>()<<<(unsigned)blocks, NL::NT, NSh::smem_bytes, s>>>(args);
-        }
-        break;
+      case 3: launch_node<true>(args, cfg.nelem, s); break;
+      case 4: launch_node<false>(args, cfg.nelem, s); break;
       default: launch<0>(args, cfg.nelem, s); break;
     }
     return cudaGetLastError();
@@ -261,7 +276,8 @@ class Engine final : public EngineBase {
       switch (variant_) {
         case 1: launch_batch<1>(args, ntiles, s); break;
         case 2: launch_batch<2>(args, ntiles, s); break;
-        case 3: node_kernel<true>()<<<(unsigned)ntiles, NL::NT, NSh::smem_bytes, s>>>(args); break;
+        case 3: launch_node_batch<true>(args, ntiles, s); break;
+        case 4: launch_node_batch<false>(args, ntiles, s); break;
         default: launch_batch<0>(args, ntiles, s); break;
       }
       return cudaGetLastError();
@@ -270,20 +286,20 @@ class Engine final : public EngineBase {
 
   int kernels_per_stage() const override { return NS ? 2 : 1; }
   int elements_per_block() const override {
-    if (variant_ == 3) return NL::EPB;
+    if (variant_ >= 3) return NL::EPB;
     return variant_ == 2 ? LaunchShape<DIM, N, 2>::EPB : LaunchShape<DIM, N, 0>::EPB;
   }
   int threads_per_block() const override {
-    if (variant_ == 3) return NL::NT;
+    if (variant_ >= 3) return NL::NT;
     return variant_ == 2 ? LaunchShape<DIM, N, 2>::NT : LaunchShape<DIM, N, 0>::NT;
   }
   size_t smem_bytes() const override {
-    if (variant_ == 3) return NSh::smem_bytes;
+    if (variant_ >= 3) return NSh::smem_bytes;
     return variant_ == 2 ? Sh<2>::smem_bytes : Sh<0>::smem_bytes;
   }
   void set_variant(int v) override { variant_ = (v >= 0 && v < num_variants()) ? v : 0; }
   int variant() const override { return variant_; }
-  int num_variants() const override { return kBatch ? 4 : 3; }
+  int num_variants() const override { return kBatch ? 5 : 3; }
 
  private:
   int variant_ = 0;

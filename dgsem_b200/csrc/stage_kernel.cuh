@@ -351,23 +351,16 @@ __device__ __forceinline__ int eidx_other_shift(const int* I, int c, int dir, in
 }
 
 // Interface or boundary flux f* at face node `line` of the face (dir, side)
-// of element `el` (surface_flux.hpp:45-271, boundary_set.hpp:70-86).
+// of element `el` (surface_flux.hpp:45-271, boundary_set.hpp:70-86), with
+// this element's state at the face node given as `so`.
 template <int DIM, int N, int VF, int SF, bool NS, int NDP>
-__device__ __forceinline__ void element_face_flux(
-    const StageArgs<N>& p, const MeshView& M, const double* us_el, const double* pr_el, const double* wv_el,
-    const int* I, int dir, int side, int line, double gamma, double t_stage, int c0, int c1,
-    int c2, double* f) {
+__device__ __forceinline__ void element_face_flux_state(
+    const StageArgs<N>& p, const MeshView& M, const FaceState<DIM>& so, const double* us_el,
+    const double* wv_el, const int* I, int dir, int side, int line, double gamma,
+    double t_stage, int c0, int c1, int c2, double* f) {
   constexpr int NV = DIM + 2, ND = ipow(N, DIM);
-  using Q = NodeSlots<DIM, VF>;
   const int own_node = line_node<DIM, N>(dir, line, side ? N - 1 : 0);
   const int opn = padn<N>(own_node);
-  FaceState<DIM> so;
-#pragma unroll
-  for (int q = 0; q < NV; ++q) so.u[q] = us_el[q * NDP + opn];
-#pragma unroll
-  for (int d = 0; d < DIM; ++d) so.v[d] = pr_el[d * NDP + opn];
-  so.p = pr_el[Q::P * NDP + opn];
-  so.a = sqrt(gamma * so.p / so.u[0]);
   const int face = 2 * dir + side;
   const int en = I[6 + face];
   if (en >= 0) {
@@ -455,6 +448,27 @@ __device__ __forceinline__ void element_face_flux(
   } else {
     surface_flux<DIM, SF>(sb, so, nrm, gamma, f);
   }
+}
+
+// element_face_flux_state with the own state taken from the line-parallel
+// kernel's shared memory (conserved tile + NodeSlots primitives).
+template <int DIM, int N, int VF, int SF, bool NS, int NDP>
+__device__ __forceinline__ void element_face_flux(
+    const StageArgs<N>& p, const MeshView& M, const double* us_el, const double* pr_el, const double* wv_el,
+    const int* I, int dir, int side, int line, double gamma, double t_stage, int c0, int c1,
+    int c2, double* f) {
+  constexpr int NV = DIM + 2;
+  using Q = NodeSlots<DIM, VF>;
+  const int opn = padn<N>(line_node<DIM, N>(dir, line, side ? N - 1 : 0));
+  FaceState<DIM> so;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) so.u[q] = us_el[q * NDP + opn];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) so.v[d] = pr_el[d * NDP + opn];
+  so.p = pr_el[Q::P * NDP + opn];
+  so.a = sqrt(gamma * so.p / so.u[0]);
+  element_face_flux_state<DIM, N, VF, SF, NS, NDP>(p, M, so, us_el, wv_el, I, dir, side, line,
+                                                   gamma, t_stage, c0, c1, c2, f);
 }
 
 // One line of direction DIR of element el: symmetric split-form pair loop

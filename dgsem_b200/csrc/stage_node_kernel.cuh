@@ -4,7 +4,7 @@
 //
 // Per block: EPB elements, EPB * n^d threads.
 //   0  element info and the coalesced u_in tile (padded shared memory);
-//   1  per-node primitives and -1/J (as stage_kernel.cuh phase 1);
+//   1  per-node flux data (NodeKernelSlots), sound speed and -1/J;
 //   2a face tasks: every (face, face node) of the block's elements computes
 //      its interface / boundary flux f* once into a shared face buffer
 //      (faces of one direction are consecutive, so warps stay uniform);
@@ -12,16 +12,41 @@
 //      n-1 other nodes of its line, sum_k Dsplit(m, k) f(u_m, u_k, (Ja_m +
 //      Ja_k)/2), accumulated in registers (each pair is evaluated by both of
 //      its nodes: twice the flux work of the symmetric line loop, but no
-//      per-direction shared buffers and ~half the registers);
+//      per-direction shared buffers and ~60 % of the registers);
 //   3  lifting of the node's face fluxes, -1/J, SSPRK3 combination, store.
 // The two-point flux is symmetric in its states, so sum_k Dsplit(m,k) f(u_m,
 // u_k) equals the reference's k > i pair loop (volume_flux.hpp:221-410)
 // up to summation order.
+//
+// Halved node data: the averages of the Kennedy-Gruber and Chandrashekar
+// fluxes, 0.5 (a + b), and the pair normal 0.5 (Ja_m + Ja_k) are formed as
+// a/2 + b/2 from values halved once per node.  Scaling by 1/2 is exact in
+// binary floating point, so each average is bit for bit the same while the
+// per-pair multiplications disappear.
 #pragma once
 
 #include "stage_kernel.cuh"
 
 namespace dgsem {
+
+// Shared-memory slots per node (the conserved density comes from the tile).
+//   KG / Chandrashekar: V (v/2, DIM), P (p/2), A (sound speed), MIJ (-1/J),
+//                       H_RHO (rho/2), X (KG: e/2; Chandrashekar: beta),
+//                       Y (Chandrashekar: |v|^2/4)
+//   Ranocha:            V (v), P (p), A, MIJ
+template <int DIM, int VF>
+struct NodeKernelSlots {
+  static constexpr bool HALF = VF != VF_RANOCHA;
+  static constexpr int V = 0;
+  static constexpr int P = DIM;
+  static constexpr int A = DIM + 1;
+  static constexpr int MIJ = DIM + 2;
+  static constexpr int H_RHO = DIM + 3;
+  static constexpr int X = DIM + 4;
+  static constexpr int Y = DIM + 5;
+  static constexpr int NQ = VF == VF_CHANDRASHEKAR ? DIM + 6
+                            : VF == VF_KENNEDY_GRUBER ? DIM + 5 : DIM + 3;
+};
 
 template <int DIM, int N, int VF, int EPB>
 struct NodeShape {
@@ -30,7 +55,7 @@ struct NodeShape {
   static constexpr int NDP = ND + ND / N;
   static constexpr int NF = ipow(N, DIM - 1);
   static constexpr int NFACE = 2 * DIM;
-  static constexpr int NQ = NodeSlots<DIM, VF>::NQ;
+  static constexpr int NQ = NodeKernelSlots<DIM, VF>::NQ;
   static constexpr int NI = 12;
   static constexpr int SM_U = EPB * NV * NDP;
   static constexpr int SM_P = EPB * NQ * NDP;
@@ -39,47 +64,130 @@ struct NodeShape {
   static constexpr size_t smem_bytes = sizeof(double) * (SM_U + SM_P + SM_F) + sizeof(int) * EPB * NI;
 };
 
+// Node data of one two-point flux evaluation (halved where NodeKernelSlots
+// says so).
+template <int DIM>
+struct NodeFluxState {
+  double rho;     // conserved density
+  double hrho;    // rho / 2
+  double v[DIM];  // v / 2 (KG, Chandrashekar) or v (Ranocha)
+  double p;       // p / 2 (KG, Chandrashekar) or p (Ranocha)
+  double x;       // KG: e / 2; Chandrashekar: beta
+  double y;       // Chandrashekar: |v|^2 / 4
+};
+
 template <int DIM, int VF>
-__device__ __forceinline__ NodeState<DIM> load_node_state(const double* U, const double* P,
-                                                          int NDP, int pn) {
-  using Q = NodeSlots<DIM, VF>;
-  NodeState<DIM> s;
+__device__ __forceinline__ NodeFluxState<DIM> load_flux_state(const double* U, const double* P,
+                                                              int NDP, int pn) {
+  using K = NodeKernelSlots<DIM, VF>;
+  NodeFluxState<DIM> s;
   s.rho = U[pn];
 #pragma unroll
-  for (int d = 0; d < DIM; ++d) s.v[d] = P[d * NDP + pn];
-  s.p = P[Q::P * NDP + pn];
-  s.beta = VF == VF_RANOCHA ? 0.0 : P[Q::BETA * NDP + pn];
-  s.kin = VF == VF_CHANDRASHEKAR ? P[Q::KIN * NDP + pn] : 0.0;
+  for (int d = 0; d < DIM; ++d) s.v[d] = P[(K::V + d) * NDP + pn];
+  s.p = P[K::P * NDP + pn];
+  s.hrho = K::HALF ? P[K::H_RHO * NDP + pn] : 0.0;
+  s.x = K::HALF ? P[K::X * NDP + pn] : 0.0;
+  s.y = VF == VF_CHANDRASHEKAR ? P[K::Y * NDP + pn] : 0.0;
   return s;
 }
 
-// Volume contribution of direction DIR to node `node` (position m on its line).
+// Two-point volume flux on node data; `n` is the full pair normal
+// (Ja_m + Ja_k)/2, `hgm1` = 1 / (2 (gamma - 1)).  Same formulas as
+// physics.cuh:volume_flux with the 1/2 factors moved into the node data.
+template <int DIM, int VF>
+__device__ __forceinline__ void node_volume_flux(const NodeFluxState<DIM>& L,
+                                                 const NodeFluxState<DIM>& R, const double* n,
+                                                 double inv_gm1, double hgm1, double* f) {
+  if constexpr (VF == VF_KENNEDY_GRUBER) {
+    const double rho_avg = L.hrho + R.hrho;
+    const double e_avg = L.x + R.x;
+    const double p_avg = L.p + R.p;
+    double va[DIM], vn_avg = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      va[d] = L.v[d] + R.v[d];
+      vn_avg += va[d] * n[d];
+    }
+    const double f1 = rho_avg * vn_avg;
+    f[0] = f1;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) f[1 + d] = f1 * va[d] + p_avg * n[d];
+    f[DIM + 1] = (rho_avg * e_avg + p_avg) * vn_avg;
+  } else if constexpr (VF == VF_CHANDRASHEKAR) {
+    double hvnL = 0.0, hvnR = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      hvnL += L.v[d] * n[d];
+      hvnR += R.v[d] * n[d];
+    }
+    double rho_mean, unused, beta_mean_unused, inv_beta_mean;
+    ln_mean_parts(L.rho, R.rho, rho_mean, unused);
+    ln_mean_parts(L.x, R.x, beta_mean_unused, inv_beta_mean);
+    const double p_mean = (L.hrho + R.hrho) / (L.x + R.x);
+    const double f1 = rho_mean * (hvnL + hvnR);
+    f[0] = f1;
+    double fe = f1 * (hgm1 * inv_beta_mean - (L.y + R.y));
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      const double va = L.v[d] + R.v[d];
+      const double fm = f1 * va + p_mean * n[d];
+      f[1 + d] = fm;
+      fe += fm * va;
+    }
+    f[DIM + 1] = fe;
+  } else {  // Ranocha on unhalved data
+    NodeState<DIM> l, r;
+    l.rho = L.rho;
+    r.rho = R.rho;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      l.v[d] = L.v[d];
+      r.v[d] = R.v[d];
+    }
+    l.p = L.p;
+    r.p = R.p;
+    l.beta = r.beta = l.kin = r.kin = 0.0;
+    volume_flux<DIM, VF_RANOCHA>(l, r, n, inv_gm1, f);
+  }
+}
+
+// Volume contribution of direction DIR to the node at padded position `pn`,
+// node index `node`, position m on its line.
 template <int DIR, int DIM, int N, int VF, int NDP>
 __device__ __forceinline__ void node_volume_direction(const StageArgs<N>& p, const MeshView& M,
                                                       const double* U, const double* P,
-                                                      const int* I, int node,
-                                                      const NodeState<DIM>& own, double* acc) {
+                                                      const int* I, int node, int pn,
+                                                      const NodeFluxState<DIM>& own,
+                                                      double hgm1, double* acc) {
   constexpr int NV = DIM + 2, ND = ipow(N, DIM);
+  constexpr bool HALF = NodeKernelSlots<DIM, VF>::HALF;
+  // node-index and padded-index strides along DIR
+  constexpr int SN = DIR == 0 ? 1 : DIR == 1 ? N : N * N;
+  constexpr int SP = DIR == 0 ? 1 : DIR == 1 ? N + 1 : N * N + N;
   const int m = DIR == 0 ? node % N : DIR == 1 ? (node / N) % N : node / (N * N);
-  const int line = DIR == 0 ? node / N
-                   : DIR == 1 ? node % N + N * (node / (N * N))
-                              : node % (N * N);
-  double ja_own[DIM];
+  const double* jrow[DIM];
+  double hja_own[DIM];
 #pragma unroll
-  for (int c = 0; c < DIM; ++c) ja_own[c] = __ldg(M.tab.ja[DIR][c] + (int64_t)I[3 + c] * ND + node);
+  for (int c = 0; c < DIM; ++c) {
+    jrow[c] = M.tab.ja[DIR][c] + (int64_t)I[3 + c] * ND + node;
+    const double j = __ldg(jrow[c]);
+    hja_own[c] = HALF ? 0.5 * j : j;
+  }
+  const double* Dm = &p.basis.Dsplit[m][0];
 #pragma unroll
   for (int o = 1; o < N; ++o) {
-    int k = m + o;
-    if (k >= N) k -= N;
-    const int nk = line_node<DIM, N>(DIR, line, k);
-    const NodeState<DIM> other = load_node_state<DIM, VF>(U, P, NDP, padn<N>(nk));
+    const bool wrap = m + o >= N;
+    const int delta = wrap ? o - N : o;  // k - m
+    const NodeFluxState<DIM> other = load_flux_state<DIM, VF>(U, P, NDP, pn + delta * SP);
     double nrm[DIM];
 #pragma unroll
-    for (int c = 0; c < DIM; ++c)
-      nrm[c] = 0.5 * (ja_own[c] + __ldg(M.tab.ja[DIR][c] + (int64_t)I[3 + c] * ND + nk));
+    for (int c = 0; c < DIM; ++c) {
+      const double jk = __ldg(jrow[c] + delta * SN);
+      nrm[c] = HALF ? hja_own[c] + 0.5 * jk : 0.5 * (hja_own[c] + jk);
+    }
     double f[NV];
-    volume_flux<DIM, VF>(own, other, nrm, p.inv_gm1, f);
-    const double dmk = p.basis.Dsplit[m][k];
+    node_volume_flux<DIM, VF>(own, other, nrm, p.inv_gm1, hgm1, f);
+    const double dmk = Dm[m + delta];
 #pragma unroll
     for (int q = 0; q < NV; ++q) acc[q] += dmk * f[q];
   }
@@ -88,7 +196,7 @@ __device__ __forceinline__ void node_volume_direction(const StageArgs<N>& p, con
 template <int DIM, int N, int VF, int SF, int EPB, bool BATCH>
 __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   using S = NodeShape<DIM, N, VF, EPB>;
-  using Q = NodeSlots<DIM, VF>;
+  using K = NodeKernelSlots<DIM, VF>;
   constexpr int NV = S::NV, ND = S::ND, NDP = S::NDP, NF = S::NF, NFACE = S::NFACE,
                 NQ = S::NQ, NI = S::NI, NT = S::NT;
   extern __shared__ double smem[];
@@ -162,20 +270,26 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   }
   __syncthreads();
 
-  // ---- phase 1: node primitives and -1/J ---------------------------------
-  for (int idx = tid; idx < ne * ND; idx += NT) {
-    const int el = idx / ND, node = idx % ND;
-    const int pn = padn<N>(node);
+  // ---- phase 1: node data, sound speed and -1/J --------------------------
+  const int el = tid / ND, node = tid % ND;
+  const bool active = el < ne;
+  const int pn = padn<N>(node);
+  if (active) {
     double u[NV];
 #pragma unroll
     for (int q = 0; q < NV; ++q) u[q] = us[(el * NV + q) * NDP + pn];
     const NodeState<DIM> s = prepare_node<DIM, VF>(u, gamma);
     double* P = pr + el * NQ * NDP + pn;
+    const double h = K::HALF ? 0.5 : 1.0;
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) P[d * NDP] = s.v[d];
-    P[Q::P * NDP] = s.p;
-    if (VF != VF_RANOCHA) P[Q::BETA * NDP] = s.beta;
-    if (VF == VF_CHANDRASHEKAR) P[Q::KIN * NDP] = s.kin;
+    for (int d = 0; d < DIM; ++d) P[(K::V + d) * NDP] = h * s.v[d];
+    P[K::P * NDP] = h * s.p;
+    P[K::A * NDP] = sqrt(gamma * s.p / u[0]);
+    if constexpr (K::HALF) {
+      P[K::H_RHO * NDP] = 0.5 * u[0];
+      P[K::X * NDP] = VF == VF_KENNEDY_GRUBER ? 0.5 * s.beta : s.beta;
+    }
+    if constexpr (VF == VF_CHANDRASHEKAR) P[K::Y * NDP] = 0.5 * s.kin;
     const int* I = info + el * NI;
     const int in = node % N, jn = (node / N) % N, kn = DIM == 3 ? node / (N * N) : 0;
     double jdet = __ldg(M.tab.jdiag[0] + I[0] * N + in);
@@ -184,23 +298,32 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
     } else {
       jdet = jdet * (__ldg(M.tab.jdiag[1] + I[1] * N + jn) * __ldg(M.tab.jdiag[2] + I[2] * N + kn));
     }
-    P[Q::MIJ * NDP] = -(1.0 / jdet);
+    P[K::MIJ * NDP] = -(1.0 / jdet);
   }
   __syncthreads();
 
   // ---- phase 2a: face fluxes, one task per (element, face, face node) ------
   for (int idx = tid; idx < ne * NFACE * NF; idx += NT) {
-    const int el = idx / (NFACE * NF);
+    const int fe = idx / (NFACE * NF);
     const int face = (idx / NF) % NFACE;
     const int fn = idx % NF;
     const int dir = face >> 1, side = face & 1;
-    const int* I = info + el * NI;
-    const double* U = us + el * NV * NDP;
-    const double* P = pr + el * NQ * NDP;
+    const int* I = info + fe * NI;
+    const double* U = us + fe * NV * NDP;
+    const double* P = pr + fe * NQ * NDP;
+    const int opn = padn<N>(line_node<DIM, N>(dir, fn, side ? N - 1 : 0));
+    FaceState<DIM> so;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) so.u[q] = U[q * NDP + opn];
+    const double g = K::HALF ? 2.0 : 1.0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) so.v[d] = g * P[(K::V + d) * NDP + opn];
+    so.p = g * P[K::P * NDP + opn];
+    so.a = P[K::A * NDP + opn];
     double f[NV];
-    element_face_flux<DIM, N, VF, SF, false, NDP>(p, M, U, P, nullptr, I, dir, side, fn, gamma,
-                                                  t_stage, c0, c1, c2, f);
-    double* F = sf + ((el * NFACE + face) * NF + fn) * NV;
+    element_face_flux_state<DIM, N, VF, SF, false, NDP>(p, M, so, U, nullptr, I, dir, side, fn,
+                                                        gamma, t_stage, c0, c1, c2, f);
+    double* F = sf + ((fe * NFACE + face) * NF + fn) * NV;
 #pragma unroll
     for (int q = 0; q < NV; ++q) F[q] = f[q];
   }
@@ -209,16 +332,16 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   double acc[NV];
 #pragma unroll
   for (int q = 0; q < NV; ++q) acc[q] = 0.0;
-  const int el = tid / ND, node = tid % ND;
-  const bool active = el < ne;
   if (active) {
     const int* I = info + el * NI;
     const double* U = us + el * NV * NDP;
     const double* P = pr + el * NQ * NDP;
-    const NodeState<DIM> own = load_node_state<DIM, VF>(U, P, NDP, padn<N>(node));
-    node_volume_direction<0, DIM, N, VF, NDP>(p, M, U, P, I, node, own, acc);
-    node_volume_direction<1, DIM, N, VF, NDP>(p, M, U, P, I, node, own, acc);
-    if constexpr (DIM == 3) node_volume_direction<2, DIM, N, VF, NDP>(p, M, U, P, I, node, own, acc);
+    const NodeFluxState<DIM> own = load_flux_state<DIM, VF>(U, P, NDP, pn);
+    const double hgm1 = 0.5 * p.inv_gm1;
+    node_volume_direction<0, DIM, N, VF, NDP>(p, M, U, P, I, node, pn, own, hgm1, acc);
+    node_volume_direction<1, DIM, N, VF, NDP>(p, M, U, P, I, node, pn, own, hgm1, acc);
+    if constexpr (DIM == 3)
+      node_volume_direction<2, DIM, N, VF, NDP>(p, M, U, P, I, node, pn, own, hgm1, acc);
   }
   __syncthreads();
   if (!active) return;
@@ -243,8 +366,7 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
       }
     }
   }
-  const int pn = padn<N>(node);
-  const double mij = pr[(el * NQ + Q::MIJ) * NDP + pn];
+  const double mij = pr[(el * NQ + K::MIJ) * NDP + pn];
   const int64_t gbase = (int64_t)(e0 + el) * NV * ND + node;
   bool bad = false;
 #pragma unroll
@@ -262,6 +384,14 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
 
 template <int DIM, int N, int VF, int SF, int EPB, bool BATCH>
 __global__ void __launch_bounds__(EPB* ipow(N, DIM)) stage_node_kernel(const StageArgs<N> p) {
+  stage_node_body<DIM, N, VF, SF, EPB, BATCH>(p);
+}
+
+// Same kernel with MINB resident blocks per SM requested from the register
+// allocator.
+template <int DIM, int N, int VF, int SF, int EPB, bool BATCH, int MINB>
+__global__ void __launch_bounds__(EPB* ipow(N, DIM), MINB)
+    stage_node_kernel_capped(const StageArgs<N> p) {
   stage_node_body<DIM, N, VF, SF, EPB, BATCH>(p);
 }
 
