@@ -662,7 +662,7 @@ def main():
                     choices=list(WORKLOADS) + ["batched", "adjoint"])
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--variant", default="auto", choices=["auto", "0", "1", "2", "3", "4"],
+    ap.add_argument("--variant", default="auto", choices=["auto", "0", "1", "2", "3", "4", "5"],
                     help="launch shape of the stage kernel (auto = autotuned)")
     args = ap.parse_args()
     if args.warmup < 3:

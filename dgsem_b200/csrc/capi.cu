@@ -625,7 +625,8 @@ dgsem_status dgsem_check_finite(dgsem_ctx* ctx) {
   if (h) {
     cudaMemsetAsync(ctx->flag, 0, sizeof(unsigned int), ctx->stream);
     cudaStreamSynchronize(ctx->stream);
-    return DGSEM_ERR_NONFINITE;
+    // bit 1: a pipelined stage kernel gave up waiting for a tile copy
+    return (h & 2u) ? DGSEM_ERR_TIMEOUT : DGSEM_ERR_NONFINITE;
   }
   return DGSEM_OK;
 }

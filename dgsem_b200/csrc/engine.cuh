@@ -14,6 +14,7 @@
 #include "br1_kernel.cuh"
 #include "stage_kernel.cuh"
 #include "stage_node_kernel.cuh"
+#include "stage_pipe_kernel.cuh"
 #include "tables.hpp"
 
 namespace dgsem {
@@ -37,9 +38,11 @@ struct EngineConfig {
 };
 
 // Launch-shape variants: 0-2 line-parallel (stage_kernel.cuh), 3-4
-// node-parallel (stage_node_kernel.cuh; split form without shock capturing
-// or viscous terms only).
-constexpr int kNumVariants = 5;
+// node-parallel (stage_node_kernel.cuh), 5 persistent node-parallel with TMA
+// tile streaming (stage_pipe_kernel.cuh; single-mesh launches).  3-5 cover
+// the split form without shock capturing or viscous terms; 5 needs an even
+// number of doubles per element (2D, or 3D with even n).
+constexpr int kNumVariants = 6;
 
 class EngineBase {
  public:
@@ -172,6 +175,38 @@ class Engine final : public EngineBase {
       node_kernel<true, CAP>()<<<(unsigned)ntiles, NL::NT, NSh::smem_bytes, s>>>(args);
   }
 
+  using PSh = PipeShape<DIM, N, VF, NL::EPB>;
+  static constexpr bool kPipe = kBatch && PSh::kSupported;
+  static auto pipe_kernel() {
+    return stage_pipe_kernel<DIM, N, VF, SF, NL::EPB, PSh::MINB>;
+  }
+  // Persistent launch: as many blocks as fit on the device at once.  Falls
+  // back to the node-parallel shape when a state pointer is not 16-byte
+  // aligned (bulk copies need it).
+  void launch_pipe(const StageArgs<N>& args, int64_t nelem, cudaStream_t s) const {
+    if constexpr (kPipe) {
+      const uintptr_t al = reinterpret_cast<uintptr_t>(args.mesh.u_in) |
+                           reinterpret_cast<uintptr_t>(args.mesh.u_n);
+      if (al & 15u) {
+        launch_node<true>(args, nelem, s);
+        return;
+      }
+      if (pipe_blocks_ == 0) {
+        int dev = 0, nsm = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pipe_kernel(), PSh::NT,
+                                                      PSh::smem_bytes);
+        pipe_blocks_ = (nsm > 0 ? nsm : 1) * (per_sm > 0 ? per_sm : 1);
+      }
+      const int64_t ntiles = (nelem + NL::EPB - 1) / NL::EPB;
+      const int64_t blocks = ntiles < pipe_blocks_ ? ntiles : pipe_blocks_;
+      pipe_kernel()<<<(unsigned)blocks, PSh::NT, PSh::smem_bytes, s>>>(args, (int)ntiles);
+    } else {
+      launch_node<true>(args, nelem, s);
+    }
+  }
+
   Engine() {
     set_attributes<0>();
     set_attributes<1>();
@@ -183,6 +218,9 @@ class Engine final : public EngineBase {
       cudaFuncSetAttribute(node_kernel<false, false>(), cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
       cudaFuncSetAttribute(node_kernel<true, false>(), cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     }
+    if constexpr (kPipe)
+      cudaFuncSetAttribute(pipe_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)PSh::smem_bytes);
   }
 
   StageArgs<N> common_args(const EngineConfig& cfg, double a, double b, double t,
@@ -249,6 +287,7 @@ class Engine final : public EngineBase {
       case 2: launch<2>(args, cfg.nelem, s); break;
       case 3: launch_node<true>(args, cfg.nelem, s); break;
       case 4: launch_node<false>(args, cfg.nelem, s); break;
+      case 5: launch_pipe(args, cfg.nelem, s); break;
       default: launch<0>(args, cfg.nelem, s); break;
     }
     return cudaGetLastError();
@@ -276,7 +315,8 @@ class Engine final : public EngineBase {
       switch (variant_) {
         case 1: launch_batch<1>(args, ntiles, s); break;
         case 2: launch_batch<2>(args, ntiles, s); break;
-        case 3: launch_node_batch<true>(args, ntiles, s); break;
+        case 3:
+        case 5: launch_node_batch<true>(args, ntiles, s); break;
         case 4: launch_node_batch<false>(args, ntiles, s); break;
         default: launch_batch<0>(args, ntiles, s); break;
       }
@@ -299,10 +339,12 @@ class Engine final : public EngineBase {
   }
   void set_variant(int v) override { variant_ = (v >= 0 && v < num_variants()) ? v : 0; }
   int variant() const override { return variant_; }
-  int num_variants() const override { return kBatch ? 5 : 3; }
+  // shape 5 exists for single-mesh launches; batched launches run it as 3
+  int num_variants() const override { return kPipe ? 6 : kBatch ? 5 : 3; }
 
  private:
   int variant_ = 0;
+  mutable int64_t pipe_blocks_ = 0;
 };
 
 }  // namespace dgsem

@@ -1,0 +1,268 @@
+// Persistent, pipelined form of the node-parallel stage kernel
+// (stage_node_kernel.cuh): the same arithmetic, with the element tiles
+// streamed through shared memory by TMA bulk copies so that HBM latency
+// overlaps computation.
+//
+// Each block loops over tiles t = blockIdx.x, blockIdx.x + gridDim.x, ...
+// (a tile = EPB consecutive elements; u[e][var][node] makes a tile one
+// contiguous range of the state).  Per tile:
+//   - u_in(t) has been requested by the previous iteration (or the prologue)
+//     as one bulk copy into `stage_in`, u_n(t) likewise into `stage_n`;
+//   - phase 1 converts stage_in into the padded tile + node data, after
+//     which one thread requests u_in(t + gridDim.x) into stage_in: the copy
+//     runs while faces, volume term and lifting of tile t are computed;
+//   - the epilogue waits for u_n(t), stores, and after the closing barrier
+//     u_n(t + gridDim.x) is requested.
+// Every wait on an mbarrier is bounded; the block votes on the outcome, and
+// on a timeout it sets bit 1 of the status flag and returns as a whole.
+// Requirements (checked by the host): u_in and u_n 16-byte aligned and an
+// even number of doubles per element (2D, or 3D with even n), so every tile
+// copy is 16-byte aligned and a multiple of 16 bytes.
+#pragma once
+
+#include "stage_node_kernel.cuh"
+#include "tma.cuh"
+
+namespace dgsem {
+
+template <int DIM, int N, int VF, int EPB>
+struct PipeShape {
+  using B = NodeShape<DIM, N, VF, EPB>;
+  static constexpr int NV = B::NV, ND = B::ND, NDP = B::NDP, NF = B::NF, NFACE = B::NFACE,
+                       NQ = B::NQ, NI = B::NI, NT = B::NT;
+  static constexpr int SM_T = EPB * NV * ND;  // one staged tile (unpadded)
+  static constexpr size_t smem_bytes =
+      sizeof(double) * (2 * SM_T + B::SM_U + B::SM_P + B::SM_F) + sizeof(int) * EPB * NI;
+  static constexpr bool kSupported = (NV * ND) % 2 == 0;
+  // resident blocks per SM allowed by shared memory (228 KB, 1 KB reserved
+  // per block), capped at 7 (72 registers per thread at 128 threads)
+  static constexpr int MINB_SMEM = int((228 * 1024) / (smem_bytes + 1024));
+  static constexpr int MINB = MINB_SMEM < 7 ? (MINB_SMEM > 0 ? MINB_SMEM : 1) : 7;
+};
+
+template <int DIM, int N, int VF, int SF, int EPB>
+__device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntiles) {
+  using S = PipeShape<DIM, N, VF, EPB>;
+  using K = NodeKernelSlots<DIM, VF>;
+  constexpr int NV = S::NV, ND = S::ND, NDP = S::NDP, NF = S::NF, NFACE = S::NFACE,
+                NQ = S::NQ, NI = S::NI, NT = S::NT;
+  extern __shared__ __align__(128) double smem_pipe[];
+  double* stage_in = smem_pipe;                    // [el][var][node], bulk-copy target
+  double* stage_n = stage_in + S::SM_T;            // [el][var][node], bulk-copy target
+  double* us = stage_n + S::SM_T;                  // [el][var][pnode]
+  double* pr = us + S::B::SM_U;                    // [el][slot][pnode]
+  double* sf = pr + S::B::SM_P;                    // [el][face][fn][var]
+  int* info = reinterpret_cast<int*>(sf + S::B::SM_F);
+  __shared__ uint64_t bar_in, bar_n;
+
+  const MeshView& M = p.mesh;
+  const int tid = threadIdx.x;
+  const int nelem = M.nelem;
+  const double gamma = p.gamma;
+  const double t_stage = p.t_dev ? (*p.t_dev + p.t) : p.t;
+  const int c0 = M.cells[0], c1 = M.cells[1], c2 = M.cells[2];
+  const bool with_n = p.a != 0.0;
+  constexpr uint32_t kElemBytes = NV * ND * sizeof(double);
+
+  auto request = [&](uint64_t* bar, double* dst, const double* src_state, int tile) {
+    const int te0 = tile * EPB;
+    const int tne = min(EPB, nelem - te0);
+    const uint32_t bytes = (uint32_t)tne * kElemBytes;
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(bar, bytes);
+    bulk_copy_g2s(dst, src_state + (int64_t)te0 * NV * ND, bytes, bar);
+  };
+
+  if (tid == 0) {
+    mbar_init(&bar_in, 1);
+    mbar_init(&bar_n, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (tid == 0 && (int)blockIdx.x < ntiles) {
+    request(&bar_in, stage_in, M.u_in, blockIdx.x);
+    if (with_n) request(&bar_n, stage_n, M.u_n, blockIdx.x);
+  }
+
+  const int el = tid / ND, node = tid % ND;
+  const int pn = padn<N>(node);
+  uint32_t phase = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, phase ^= 1u) {
+    const int e0 = t * EPB;
+    const int ne = min(EPB, nelem - e0);
+    const bool active = el < ne;
+
+    // ---- element info ------------------------------------------------------
+    if (tid < ne) {
+      const int e = e0 + tid;
+      int ijk[3];
+      ijk[0] = e % c0;
+      ijk[1] = DIM == 2 ? e / c0 : (e / c0) % c1;
+      ijk[2] = DIM == 2 ? 0 : e / (c0 * c1);
+      int* I = info + tid * NI;
+      I[0] = ijk[0];
+      I[1] = ijk[1];
+      I[2] = ijk[2];
+      if (DIM == 2) {
+        I[3] = ijk[1];
+        I[4] = ijk[0];
+        I[5] = 0;
+      } else {
+        I[3] = ijk[1] + c1 * ijk[2];
+        I[4] = ijk[0] + c0 * ijk[2];
+        I[5] = ijk[0] + c0 * ijk[1];
+      }
+      const int cells[3] = {c0, c1, c2};
+#pragma unroll
+      for (int face = 0; face < NFACE; ++face) {
+        const int dir = face >> 1, side = face & 1;
+        int pos = ijk[dir] + (side ? 1 : -1);
+        int nbr = -1;
+        if (pos < 0 || pos >= cells[dir]) {
+          if (M.periodic[dir]) pos = (pos + cells[dir]) % cells[dir];
+          else pos = -1;
+        }
+        if (pos >= 0) {
+          int q[3] = {ijk[0], ijk[1], ijk[2]};
+          q[dir] = pos;
+          nbr = DIM == 2 ? q[0] + c0 * q[1] : q[0] + c0 * (q[1] + c1 * q[2]);
+        }
+        I[6 + face] = nbr;
+      }
+    }
+    // the block agrees on a timeout (vote) so that all of it leaves together
+    if (__syncthreads_or(!mbar_wait_bounded(&bar_in, phase))) {
+      if (tid == 0) atomicOr(p.nonfinite, 2u);
+      return;
+    }
+
+    // ---- phase 1: tile -> padded tile + node data, sound speed, -1/J -------
+    if (active) {
+      double u[NV];
+#pragma unroll
+      for (int q = 0; q < NV; ++q) {
+        u[q] = stage_in[(el * NV + q) * ND + node];
+        us[(el * NV + q) * NDP + pn] = u[q];
+      }
+      const NodeState<DIM> s = prepare_node<DIM, VF>(u, gamma);
+      double* P = pr + el * NQ * NDP + pn;
+      const double h = K::HALF ? 0.5 : 1.0;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) P[(K::V + d) * NDP] = h * s.v[d];
+      P[K::P * NDP] = h * s.p;
+      P[K::A * NDP] = sqrt(gamma * s.p / u[0]);
+      if constexpr (K::HALF) {
+        P[K::H_RHO * NDP] = 0.5 * u[0];
+        P[K::X * NDP] = VF == VF_KENNEDY_GRUBER ? 0.5 * s.beta : s.beta;
+      }
+      if constexpr (VF == VF_CHANDRASHEKAR) P[K::Y * NDP] = 0.5 * s.kin;
+      const int* I = info + el * NI;
+      const int in = node % N, jn = (node / N) % N, kn = DIM == 3 ? node / (N * N) : 0;
+      double jdet = __ldg(M.tab.jdiag[0] + I[0] * N + in);
+      if (DIM == 2) {
+        jdet = jdet * __ldg(M.tab.jdiag[1] + I[1] * N + jn);
+      } else {
+        jdet = jdet * (__ldg(M.tab.jdiag[1] + I[1] * N + jn) *
+                       __ldg(M.tab.jdiag[2] + I[2] * N + kn));
+      }
+      P[K::MIJ * NDP] = -(1.0 / jdet);
+    }
+    __syncthreads();
+    // stage_in is consumed: request the next tile's u_in
+    if (tid == 0 && t + (int)gridDim.x < ntiles)
+      request(&bar_in, stage_in, M.u_in, t + gridDim.x);
+
+    // ---- phase 2a: face fluxes ---------------------------------------------
+    for (int idx = tid; idx < ne * NFACE * NF; idx += NT) {
+      const int fe = idx / (NFACE * NF);
+      const int face = (idx / NF) % NFACE;
+      const int fn = idx % NF;
+      const int dir = face >> 1, side = face & 1;
+      const int* I = info + fe * NI;
+      const double* U = us + fe * NV * NDP;
+      const double* P = pr + fe * NQ * NDP;
+      const int opn = padn<N>(line_node<DIM, N>(dir, fn, side ? N - 1 : 0));
+      FaceState<DIM> so;
+#pragma unroll
+      for (int q = 0; q < NV; ++q) so.u[q] = U[q * NDP + opn];
+      const double g = K::HALF ? 2.0 : 1.0;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) so.v[d] = g * P[(K::V + d) * NDP + opn];
+      so.p = g * P[K::P * NDP + opn];
+      so.a = P[K::A * NDP + opn];
+      double f[NV];
+      element_face_flux_state<DIM, N, VF, SF, false, NDP>(p, M, so, U, nullptr, I, dir, side, fn,
+                                                          gamma, t_stage, c0, c1, c2, f);
+      double* F = sf + ((fe * NFACE + face) * NF + fn) * NV;
+#pragma unroll
+      for (int q = 0; q < NV; ++q) F[q] = f[q];
+    }
+
+    // ---- phase 2b: volume term ---------------------------------------------
+    double acc[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) acc[q] = 0.0;
+    if (active) {
+      const int* I = info + el * NI;
+      const double* U = us + el * NV * NDP;
+      const double* P = pr + el * NQ * NDP;
+      const NodeFluxState<DIM> own = load_flux_state<DIM, VF>(U, P, NDP, pn);
+      const double hgm1 = 0.5 * p.inv_gm1;
+      node_volume_direction<0, DIM, N, VF, NDP>(p, M, U, P, I, node, pn, own, hgm1, acc);
+      node_volume_direction<1, DIM, N, VF, NDP>(p, M, U, P, I, node, pn, own, hgm1, acc);
+      if constexpr (DIM == 3)
+        node_volume_direction<2, DIM, N, VF, NDP>(p, M, U, P, I, node, pn, own, hgm1, acc);
+    }
+    __syncthreads();
+
+    // ---- phase 3: lifting, -1/J, SSPRK3 combination, store -----------------
+    if (with_n && __syncthreads_or(!mbar_wait_bounded(&bar_n, phase))) {
+      if (tid == 0) atomicOr(p.nonfinite, 2u);
+      return;
+    }
+    if (active) {
+      const int pos[3] = {node % N, (node / N) % N, DIM == 3 ? node / (N * N) : 0};
+#pragma unroll
+      for (int dir = 0; dir < DIM; ++dir) {
+        const int line = dir == 0 ? node / N
+                         : dir == 1 ? node % N + N * (node / (N * N))
+                                    : node % (N * N);
+        if (pos[dir] == 0) {
+          const double* F = sf + ((el * NFACE + 2 * dir) * NF + line) * NV;
+#pragma unroll
+          for (int q = 0; q < NV; ++q) acc[q] -= F[q] * p.basis.lhat_l0;
+        }
+        if (pos[dir] == N - 1) {
+          const double* F = sf + ((el * NFACE + 2 * dir + 1) * NF + line) * NV;
+#pragma unroll
+          for (int q = 0; q < NV; ++q) acc[q] += F[q] * p.basis.lhat_rN;
+        }
+      }
+      const double mij = pr[(el * NQ + K::MIJ) * NDP + pn];
+      const int64_t gbase = (int64_t)(e0 + el) * NV * ND + node;
+      bool bad = false;
+#pragma unroll
+      for (int q = 0; q < NV; ++q) {
+        const double du = acc[q] * mij;
+        double val = M.c * du;
+        if (p.b != 0.0) val = p.b * us[(el * NV + q) * NDP + pn] + val;
+        if (with_n) val = p.a * stage_n[(el * NV + q) * ND + node] + val;
+        bad |= !isfinite(val);
+        M.out[gbase + (int64_t)q * ND] = val;
+      }
+      if (bad) atomicOr(p.nonfinite, 1u);
+    }
+    __syncthreads();
+    // stage_n, padded tile, node data and face buffer are free again
+    if (tid == 0 && with_n && t + (int)gridDim.x < ntiles)
+      request(&bar_n, stage_n, M.u_n, t + gridDim.x);
+  }
+}
+
+template <int DIM, int N, int VF, int SF, int EPB, int MINB>
+__global__ void __launch_bounds__(EPB* ipow(N, DIM), MINB)
+    stage_pipe_kernel(const StageArgs<N> p, int ntiles) {
+  stage_pipe_body<DIM, N, VF, SF, EPB>(p, ntiles);
+}
+
+}  // namespace dgsem

@@ -262,18 +262,21 @@ dgsem_status dgsem_from_reference_layout(dgsem_ctx* ctx, const double* u_ref,
 
 /* Non-finite detection: every stage kernel ORs a device flag when it writes a
  * NaN/Inf.  This call synchronises the stream, returns DGSEM_ERR_NONFINITE if
- * the flag is set, and clears it. */
+ * the flag is set (DGSEM_ERR_TIMEOUT if a pipelined stage kernel gave up
+ * waiting for a tile copy), and clears it. */
 dgsem_status dgsem_check_finite(dgsem_ctx* ctx);
 
 /* Launch-shape autotuner (no reference counterpart; the reference has one
- * fixed Kokkos launch shape).  The fused stage kernel has up to 5 launch
+ * fixed Kokkos launch shape).  The fused stage kernel has up to 6 launch
  * shapes: 0-2 line-parallel (elements per block, register cap; bitwise
- * identical results), 3-4 node-parallel with and without a register cap
- * (split form without shock capturing or viscous terms only; same fluxes,
- * different summation order: agrees with 0-2 to rounding).  dgsem_autotune times each available shape on this context's
+ * identical results), 3-4 node-parallel with and without a register cap, 5
+ * persistent node-parallel streaming element tiles through shared memory
+ * with bulk copies (3-5: split form without shock capturing or viscous
+ * terms; 5: 2D or even n in 3D; same results as 3; 3-5 agree with 0-2 to
+ * rounding: same fluxes, different summation order).  dgsem_autotune times each available shape on this context's
  * mesh with state u (RHS launches into a context temporary; u is not
  * modified), keeps the fastest and returns it in *chosen (may be NULL);
- * times_ms (5 doubles, may be NULL; 0 for an unavailable shape) receives the
+ * times_ms (6 doubles, may be NULL; 0 for an unavailable shape) receives the
  * mean launch times and forces re-timing.  Choices are
  * cached per (scheme, degree, element count) for the process and, when the
  * environment variable DGSEM_TUNING_FILE names a file, persisted there.

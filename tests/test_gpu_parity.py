@@ -318,13 +318,14 @@ def test_launch_variants(name, cuda):
         # order (each pair evaluated by both of its nodes); 3 and 4 differ
         # only in the register cap and give the same bits
         node_outs = []
-        for v in (3, 4):
+        for v in (3, 4, 5):
             solver.set_launch_variant(v)
             du3 = torch.empty_like(u)
             solver.rhs(u, du3, 0.05)
             node_outs.append(du3)
         torch.cuda.synchronize()
         assert torch.equal(node_outs[0], node_outs[1])
+        assert torch.equal(node_outs[0], node_outs[2])
         a, b = node_outs[0].cpu().numpy(), outs[0].cpu().numpy()
         assert rel_linf(a, b) <= RTOL
         assert rel_linf(dev_to_ref(a, solver.mesh.n_cells), do.rhs(s, u_ref, 0.05)) <= RTOL
@@ -333,7 +334,7 @@ def test_launch_variants(name, cuda):
             solver.set_launch_variant(3)
     chosen, times = solver.autotune(u, retime=True)
     torch.cuda.synchronize()
-    assert chosen in ((0, 1, 2, 3, 4) if node_variant else (0, 1, 2))
+    assert chosen in ((0, 1, 2, 3, 4, 5) if node_variant else (0, 1, 2))
     assert all(t > 0.0 for t in times[:5 if node_variant else 3])
     assert torch.equal(u, u_copy)
     du = torch.empty_like(u)
