@@ -80,9 +80,21 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profile_traffic(workload: str):
+# stage kernel launched by each launch shape (dgsem_autotune / --variant)
+VARIANT_KERNELS = {
+    0: "stage_kernel", 1: "stage_kernel", 2: "stage_kernel",
+    3: "stage_node_kernel", 4: "stage_node_kernel", 5: "stage_pipe_kernel",
+}
+KERNEL_DESCRIPTIONS = {
+    "stage_kernel": "stage_kernel (line-parallel fused RHS + SSPRK3 stage)",
+    "stage_node_kernel": "stage_node_kernel (node-parallel fused RHS + SSPRK3 stage)",
+    "stage_pipe_kernel": "stage_pipe_kernel (persistent node-parallel, TMA tile streaming)",
+}
+
+
+def profile_traffic(workload: str, kernel: str = "stage_kernel"):
     """Per-launch DRAM bytes of the stage kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", f"stage_kernel_{workload}.md")
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
     try:
         with open(path) as f:
             for line in f:
@@ -344,7 +356,8 @@ def run_device_arm(args):
     mean_stage_s = sum(sum(x) for x in stage_ms) / (3 * args.steps) * 1e-3
     achieved = dofs * bpd / mean_stage_s / 1e9
     peak, peak_kind = measured_peak()
-    traffic = profile_traffic(name)
+    kernel = VARIANT_KERNELS.get(variant, "stage_kernel")
+    traffic = profile_traffic(name, kernel)
 
     # e2e through the host-buffer C-ABI entry point (pinned host state)
     n_e2e = max(3, min(args.steps, 200))
@@ -389,7 +402,7 @@ def run_device_arm(args):
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs"
                      if peak_kind == "measured" else "fallback 6650 GB/s",
-                     "kernel": "stage_kernel (fused RHS + SSPRK3 stage)",
+                     "kernel": KERNEL_DESCRIPTIONS[kernel],
                      "algorithmic_bytes_per_launch": dofs * bpd},
         "e2e": {"value": e2e_value, "unit": "DOF-updates/s", "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes, "steps": n_e2e,

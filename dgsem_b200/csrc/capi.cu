@@ -687,13 +687,17 @@ std::string tune_key(int ndims, int n, int vf, int sf, int hg, int ns, int64_t n
   return k.str();
 }
 
-// Times `launch` (one kernel launch sequence on `s`) for each variant of
-// `eng`; returns the fastest variant and optionally the mean times.
+// Times `launch` (one SSPRK3 step on `s`) for each variant of `eng`: one
+// warm-up, then `reps` timed launches, each preceded (outside the timed
+// region) by a write of `flush_bytes` to `flush` when given, which evicts L2
+// so that every timed step streams its states from HBM.  Returns the fastest
+// variant and optionally the mean times.
 template <class Launch>
-int time_variants(EngineBase* eng, cudaStream_t s, Launch&& launch, double* times_ms) {
-  cudaEvent_t a, b;
-  cudaEventCreate(&a);
-  cudaEventCreate(&b);
+int time_variants(EngineBase* eng, cudaStream_t s, Launch&& launch, double* times_ms,
+                  void* flush, size_t flush_bytes) {
+  constexpr int reps = 5;
+  cudaEvent_t ev[2 * reps];
+  for (auto& e : ev) cudaEventCreate(&e);
   int best = 0;
   float best_ms = 1e30f;
   for (int v = 0; v < kNumVariants; ++v) {
@@ -703,13 +707,19 @@ int time_variants(EngineBase* eng, cudaStream_t s, Launch&& launch, double* time
     }
     eng->set_variant(v);
     launch();  // warm-up
-    cudaEventRecord(a, s);
-    constexpr int reps = 5;
-    for (int r = 0; r < reps; ++r) launch();
-    cudaEventRecord(b, s);
-    cudaEventSynchronize(b);
+    for (int r = 0; r < reps; ++r) {
+      if (flush) cudaMemsetAsync(flush, r & 0xff, flush_bytes, s);
+      cudaEventRecord(ev[2 * r], s);
+      launch();
+      cudaEventRecord(ev[2 * r + 1], s);
+    }
+    cudaEventSynchronize(ev[2 * reps - 1]);
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, a, b);
+    for (int r = 0; r < reps; ++r) {
+      float m = 0.f;
+      cudaEventElapsedTime(&m, ev[2 * r], ev[2 * r + 1]);
+      ms += m;
+    }
     ms /= reps;
     if (times_ms) times_ms[v] = ms;
     if (ms < best_ms) {
@@ -717,8 +727,7 @@ int time_variants(EngineBase* eng, cudaStream_t s, Launch&& launch, double* time
       best = v;
     }
   }
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
+  for (auto& e : ev) cudaEventDestroy(e);
   return best;
 }
 
@@ -736,10 +745,12 @@ dgsem_status dgsem_autotune(dgsem_ctx* ctx, const double* u, int* chosen, double
   using namespace dgsem::tune_detail;
   if (!ctx || !u) return DGSEM_ERR_INVALID_ARG;
   const EngineConfig& c = ctx->cfg;
+  const bool warm = std::getenv("DGSEM_AUTOTUNE_WARM") != nullptr;
   const std::string key =
       tune_key(c.ndims, c.n, ctx->scheme.volume_flux, ctx->scheme.surface_flux,
                ctx->scheme.volume_integral, ctx->scheme.equation == DGSEM_NAVIER_STOKES_2D,
-               c.nelem);
+               c.nelem) +
+      (warm ? "_warm" : "_cold");
   std::lock_guard<std::mutex> lock(tune_mutex());
   auto it = tune_cache().find(key);
   if (it != tune_cache().end() && !times_ms) {
@@ -747,12 +758,32 @@ dgsem_status dgsem_autotune(dgsem_ctx* ctx, const double* u, int* chosen, double
     if (chosen) *chosen = it->second;
     return DGSEM_OK;
   }
+  // L2 eviction buffer (twice the 126 MB L2), released before returning
+  void* flush = nullptr;
+  const size_t flush_bytes = size_t(256) << 20;
+  if (!warm && cudaMalloc(&flush, flush_bytes) != cudaSuccess) {
+    cudaGetLastError();
+    flush = nullptr;
+  }
+  // one SSPRK3 step from u into the context temporaries (u is not modified)
   cudaError_t err = cudaSuccess;
+  const double dt = 1.0e-6;
   const int best = time_variants(ctx->engine.get(), ctx->stream, [&]() {
-    cudaError_t e = ctx->engine->stage(ctx->cfg, nullptr, u, ctx->tmp1, 0.0, 0.0, 1.0, 0.0,
-                                       nullptr, nullptr, ctx->stream);
+    EngineBase* eng = ctx->engine.get();
+    cudaError_t e = eng->stage(ctx->cfg, nullptr, u, ctx->tmp1, 0.0, 1.0, dt, 0.0, nullptr,
+                               nullptr, ctx->stream);
+    if (e == cudaSuccess)
+      e = eng->stage(ctx->cfg, u, ctx->tmp1, ctx->tmp2, 3.0 / 4.0, 1.0 / 4.0, dt / 4.0, dt,
+                     nullptr, nullptr, ctx->stream);
+    if (e == cudaSuccess)
+      e = eng->stage(ctx->cfg, u, ctx->tmp2, ctx->tmp1, 1.0 / 3.0, 2.0 / 3.0, 2.0 * dt / 3.0,
+                     0.5 * dt, nullptr, nullptr, ctx->stream);
     if (e != cudaSuccess) err = e;
-  }, times_ms);
+  }, times_ms, flush, flush_bytes);
+  if (flush) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(flush);
+  }
   if (err != cudaSuccess) return DGSEM_ERR_CUDA;
   ctx->engine->set_variant(best);
   tune_store(key, best);

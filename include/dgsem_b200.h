@@ -273,13 +273,17 @@ dgsem_status dgsem_check_finite(dgsem_ctx* ctx);
  * persistent node-parallel streaming element tiles through shared memory
  * with bulk copies (3-5: split form without shock capturing or viscous
  * terms; 5: 2D or even n in 3D; same results as 3; 3-5 agree with 0-2 to
- * rounding: same fluxes, different summation order).  dgsem_autotune times each available shape on this context's
- * mesh with state u (RHS launches into a context temporary; u is not
- * modified), keeps the fastest and returns it in *chosen (may be NULL);
- * times_ms (6 doubles, may be NULL; 0 for an unavailable shape) receives the
- * mean launch times and forces re-timing.  Choices are
- * cached per (scheme, degree, element count) for the process and, when the
- * environment variable DGSEM_TUNING_FILE names a file, persisted there.
+ * rounding: same fluxes, different summation order).  dgsem_autotune times
+ * one SSPRK3 step from state u (into the context temporaries; u is not
+ * modified) with each available shape, keeps the fastest and returns it in
+ * *chosen (may be NULL); times_ms (6 doubles, may be NULL; 0 for an
+ * unavailable shape) receives the mean step times and forces re-timing.
+ * Every timed step is preceded by an L2 eviction (a 256 MiB temporary
+ * buffer, freed before returning), i.e. states stream from HBM as in large
+ * runs; with the environment variable DGSEM_AUTOTUNE_WARM set, steps are
+ * timed back to back instead (L2-resident small meshes).  Choices are cached
+ * per (scheme, degree, element count, timing mode) for the process and, when
+ * the environment variable DGSEM_TUNING_FILE names a file, persisted there.
  * Synchronous. */
 dgsem_status dgsem_autotune(dgsem_ctx* ctx, const double* u, int* chosen,
                             double* times_ms);
