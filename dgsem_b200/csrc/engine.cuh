@@ -162,17 +162,21 @@ class Engine final : public EngineBase {
     else
       return stage_node_kernel<DIM, N, VF, SF, NL::EPB, B>;
   }
+  // launches without u_n (a == 0) request the smaller shared-memory size
+  static size_t node_smem(const StageArgs<N>& args) {
+    return args.a != 0.0 ? NSh::smem_bytes : NSh::smem_bytes_base;
+  }
   template <bool CAP>
   void launch_node(const StageArgs<N>& args, int64_t nelem, cudaStream_t s) const {
     if constexpr (kBatch) {
       const int64_t blocks = (nelem + NL::EPB - 1) / NL::EPB;
-      node_kernel<false, CAP>()<<<(unsigned)blocks, NL::NT, NSh::smem_bytes, s>>>(args);
+      node_kernel<false, CAP>()<<<(unsigned)blocks, NL::NT, node_smem(args), s>>>(args);
     }
   }
   template <bool CAP>
   void launch_node_batch(const StageArgs<N>& args, int ntiles, cudaStream_t s) const {
     if constexpr (kBatch)
-      node_kernel<true, CAP>()<<<(unsigned)ntiles, NL::NT, NSh::smem_bytes, s>>>(args);
+      node_kernel<true, CAP>()<<<(unsigned)ntiles, NL::NT, node_smem(args), s>>>(args);
   }
 
   using PSh = PipeShape<DIM, N, VF, NL::EPB>;

@@ -13,7 +13,10 @@
 //      Ja_k)/2), accumulated in registers (each pair is evaluated by both of
 //      its nodes: twice the flux work of the symmetric line loop, but no
 //      per-direction shared buffers and ~60 % of the registers);
-//   3  lifting of the node's face fluxes, -1/J, SSPRK3 combination, store.
+//   3  lifting of the node's face fluxes, -1/J, SSPRK3 combination, store;
+//      the u_n tile of the combination is requested at kernel start as one
+//      bulk (TMA) copy into shared memory (16-byte-aligned states with an
+//      even number of doubles per element; otherwise read directly).
 // The two-point flux is symmetric in its states, so sum_k Dsplit(m,k) f(u_m,
 // u_k) equals the reference's k > i pair loop (volume_flux.hpp:221-410)
 // up to summation order.
@@ -26,6 +29,7 @@
 #pragma once
 
 #include "stage_kernel.cuh"
+#include "tma.cuh"
 
 namespace dgsem {
 
@@ -60,8 +64,15 @@ struct NodeShape {
   static constexpr int SM_U = EPB * NV * NDP;
   static constexpr int SM_P = EPB * NQ * NDP;
   static constexpr int SM_F = EPB * NFACE * NF * NV;  // f* [el][face][fn][var]
+  // staged u_n tile (one bulk copy) when a tile is a multiple of 16 bytes;
+  // placed last so that launches without u_n (stage 1, RHS) can request
+  // smem_bytes_base and leave the rest of the SM's storage to L1
+  static constexpr int SM_N = (NV * ND) % 2 == 0 ? EPB * NV * ND : 0;
   static constexpr int NT = EPB * ND;
-  static constexpr size_t smem_bytes = sizeof(double) * (SM_U + SM_P + SM_F) + sizeof(int) * EPB * NI;
+  static constexpr size_t smem_bytes_base =
+      sizeof(double) * (SM_U + SM_P + SM_F) + sizeof(int) * EPB * NI;
+  static constexpr size_t off_n_bytes = (smem_bytes_base + 15) / 16 * 16;
+  static constexpr size_t smem_bytes = off_n_bytes + sizeof(double) * SM_N;
 };
 
 // Node data of one two-point flux evaluation (halved where NodeKernelSlots
@@ -199,11 +210,13 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   using K = NodeKernelSlots<DIM, VF>;
   constexpr int NV = S::NV, ND = S::ND, NDP = S::NDP, NF = S::NF, NFACE = S::NFACE,
                 NQ = S::NQ, NI = S::NI, NT = S::NT;
-  extern __shared__ double smem[];
-  double* us = smem;             // [el][var][pnode]
+  extern __shared__ __align__(128) double smem_node[];
+  double* us = smem_node;        // [el][var][pnode]
   double* pr = us + S::SM_U;     // [el][slot][pnode]
   double* sf = pr + S::SM_P;     // [el][face][fn][var]
   int* info = reinterpret_cast<int*>(sf + S::SM_F);
+  // [el][var][node] u_n tile (bulk-copy target; present when p.a != 0)
+  double* stage_n = reinterpret_cast<double*>(reinterpret_cast<char*>(smem_node) + S::off_n_bytes);
 
   const int tid = threadIdx.x;
   __shared__ MeshView mesh_s;
@@ -222,6 +235,20 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   const double gamma = p.gamma;
   const double t_stage = p.t_dev ? (*p.t_dev + p.t) : p.t;
   const int c0 = M.cells[0], c1 = M.cells[1], c2 = M.cells[2];
+
+  // The epilogue's u_n tile is requested now as one bulk copy so that it
+  // arrives while the block computes (block-uniform decision).
+  __shared__ uint64_t bar_n;
+  bool bulk_n = false;
+  if constexpr (S::SM_N > 0)
+    bulk_n = p.a != 0.0 && (reinterpret_cast<uintptr_t>(M.u_n) & 15u) == 0;
+  if (bulk_n && tid == 0) {
+    const uint32_t bytes = (uint32_t)ne * NV * ND * sizeof(double);
+    mbar_init(&bar_n, 1);
+    mbar_fence_init();
+    mbar_arrive_expect_tx(&bar_n, bytes);
+    bulk_copy_g2s(stage_n, M.u_n + (int64_t)e0 * NV * ND, bytes, &bar_n);
+  }
 
   // ---- phase 0: element info and the u_in tile --------------------------
   for (int el = tid; el < ne; el += NT) {
@@ -344,6 +371,11 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
       node_volume_direction<2, DIM, N, VF, NDP>(p, M, U, P, I, node, pn, own, hgm1, acc);
   }
   __syncthreads();
+  // the block agrees on a timeout (vote) so that all of it leaves together
+  if (bulk_n && __syncthreads_or(!mbar_wait_bounded(&bar_n, 0))) {
+    if (tid == 0) atomicOr(p.nonfinite, 2u);
+    return;
+  }
   if (!active) return;
 
   // ---- phase 3: lifting (surface_integral.hpp:35-154), -1/J, SSPRK3 --------
@@ -375,7 +407,8 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
     const int64_t gi = gbase + (int64_t)q * ND;
     double val = M.c * du;
     if (p.b != 0.0) val = p.b * us[(el * NV + q) * NDP + pn] + val;
-    if (p.a != 0.0) val = p.a * M.u_n[gi] + val;
+    if (p.a != 0.0)
+      val = p.a * (bulk_n ? stage_n[(el * NV + q) * ND + node] : M.u_n[gi]) + val;
     bad |= !isfinite(val);
     M.out[gi] = val;
   }
