@@ -153,14 +153,17 @@ class Engine final : public EngineBase {
                            (int)Sh<V>::smem_bytes);
   }
 
+  // node-parallel shapes: split form with or without shock capturing (not
+  // Navier-Stokes); batched node launches without shock capturing only
+  static constexpr bool kNode = !NS;
   using NL = NodeLaunch<DIM, N>;
-  using NSh = NodeShape<DIM, N, VF, NL::EPB>;
+  using NSh = NodeShape<DIM, N, VF, NL::EPB, HG>;
   template <bool B, bool CAP>
   static auto node_kernel() {
     if constexpr (CAP)
-      return stage_node_kernel_capped<DIM, N, VF, SF, NL::EPB, B, NL::MINB>;
+      return stage_node_kernel_capped<DIM, N, VF, SF, NL::EPB, B, NL::MINB, HG>;
     else
-      return stage_node_kernel<DIM, N, VF, SF, NL::EPB, B>;
+      return stage_node_kernel<DIM, N, VF, SF, NL::EPB, B, HG>;
   }
   // launches without u_n (a == 0) request the smaller shared-memory size
   static size_t node_smem(const StageArgs<N>& args) {
@@ -168,7 +171,7 @@ class Engine final : public EngineBase {
   }
   template <bool CAP>
   void launch_node(const StageArgs<N>& args, int64_t nelem, cudaStream_t s) const {
-    if constexpr (kBatch) {
+    if constexpr (kNode) {
       const int64_t blocks = (nelem + NL::EPB - 1) / NL::EPB;
       node_kernel<false, CAP>()<<<(unsigned)blocks, NL::NT, node_smem(args), s>>>(args);
     }
@@ -215,11 +218,14 @@ class Engine final : public EngineBase {
     set_attributes<0>();
     set_attributes<1>();
     set_attributes<2>();
-    if constexpr (kBatch) {
+    if constexpr (kNode) {
       const int sm = (int)NSh::smem_bytes;
       cudaFuncSetAttribute(node_kernel<false, true>(), cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-      cudaFuncSetAttribute(node_kernel<true, true>(), cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
       cudaFuncSetAttribute(node_kernel<false, false>(), cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    }
+    if constexpr (kBatch) {
+      const int sm = (int)NSh::smem_bytes;
+      cudaFuncSetAttribute(node_kernel<true, true>(), cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
       cudaFuncSetAttribute(node_kernel<true, false>(), cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     }
     if constexpr (kPipe)
@@ -344,7 +350,7 @@ class Engine final : public EngineBase {
   void set_variant(int v) override { variant_ = (v >= 0 && v < num_variants()) ? v : 0; }
   int variant() const override { return variant_; }
   // shape 5 exists for single-mesh launches; batched launches run it as 3
-  int num_variants() const override { return kPipe ? 6 : kBatch ? 5 : 3; }
+  int num_variants() const override { return kPipe ? 6 : kNode ? 5 : 3; }
 
  private:
   int variant_ = 0;

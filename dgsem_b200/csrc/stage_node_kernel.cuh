@@ -1,6 +1,7 @@
-// Node-parallel form of the fused stage kernel (split form without shock
-// capturing or viscous terms): the same right-hand side and SSPRK3 epilogue
-// as stage_kernel.cuh, organised for occupancy instead of minimal flux count.
+// Node-parallel form of the fused stage kernel (split form, optionally with
+// Hennemann-Gassner shock capturing in 2D; no viscous terms): the same
+// right-hand side and SSPRK3 epilogue as stage_kernel.cuh, organised for
+// occupancy instead of minimal flux count.
 //
 // Per block: EPB elements, EPB * n^d threads.
 //   0  element info and the coalesced u_in tile (padded shared memory);
@@ -52,7 +53,7 @@ struct NodeKernelSlots {
                             : VF == VF_KENNEDY_GRUBER ? DIM + 5 : DIM + 3;
 };
 
-template <int DIM, int N, int VF, int EPB>
+template <int DIM, int N, int VF, int EPB, bool HG = false>
 struct NodeShape {
   static constexpr int NV = DIM + 2;
   static constexpr int ND = ipow(N, DIM);
@@ -63,14 +64,18 @@ struct NodeShape {
   static constexpr int NI = 12;
   static constexpr int SM_U = EPB * NV * NDP;
   static constexpr int SM_P = EPB * NQ * NDP;
-  static constexpr int SM_F = EPB * NFACE * NF * NV;  // f* [el][face][fn][var]
+  // f* [el][face][fn][var]; with shock capturing also the indicator scratch
+  static constexpr int SM_F0 = EPB * NFACE * NF * NV;
+  static constexpr int SM_F = HG && 3 * EPB * ND > SM_F0 ? 3 * EPB * ND : SM_F0;
+  static constexpr int SM_A = HG ? EPB : 0;        // alpha per element
+  static constexpr int SM_VINV = HG ? N * N : 0;   // inverse Legendre Vandermonde
   // staged u_n tile (one bulk copy) when a tile is a multiple of 16 bytes;
   // placed last so that launches without u_n (stage 1, RHS) can request
   // smem_bytes_base and leave the rest of the SM's storage to L1
   static constexpr int SM_N = (NV * ND) % 2 == 0 ? EPB * NV * ND : 0;
   static constexpr int NT = EPB * ND;
   static constexpr size_t smem_bytes_base =
-      sizeof(double) * (SM_U + SM_P + SM_F) + sizeof(int) * EPB * NI;
+      sizeof(double) * (SM_U + SM_P + SM_F + SM_A + SM_VINV) + sizeof(int) * EPB * NI;
   static constexpr size_t off_n_bytes = (smem_bytes_base + 15) / 16 * 16;
   static constexpr size_t smem_bytes = off_n_bytes + sizeof(double) * SM_N;
 };
@@ -204,9 +209,59 @@ __device__ __forceinline__ void node_volume_direction(const StageArgs<N>& p, con
   }
 }
 
-template <int DIM, int N, int VF, int SF, int EPB, bool BATCH>
+// Hennemann-Gassner FV subcell contribution of direction DIR to the node
+// (volume_flux.hpp:457-509): LLF on the subcell normals at the node's two
+// subcell interfaces, weighted by alpha / w_m (each interface flux is
+// evaluated by both of its nodes).
+template <int DIR, int DIM, int N, int VF, int NDP>
+__device__ __forceinline__ void node_fv_direction(const StageArgs<N>& p, const MeshView& M,
+                                                  const double* U, const double* P,
+                                                  const int* I, int node, double alpha,
+                                                  double* acc) {
+  constexpr int NV = DIM + 2;
+  using K = NodeKernelSlots<DIM, VF>;
+  static_assert(DIM == 2, "shock capturing: 2D");
+  const int m = DIR == 0 ? node % N : node / N;
+  const int line = DIR == 0 ? node / N : node % N;
+  auto state = [&](int k) {
+    const int pk = padn<N>(line_node<DIM, N>(DIR, line, k));
+    FaceState<DIM> st;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) st.u[q] = U[q * NDP + pk];
+    const double g = K::HALF ? 2.0 : 1.0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) st.v[d] = g * P[(K::V + d) * NDP + pk];
+    st.p = g * P[K::P * NDP + pk];
+    st.a = P[K::A * NDP + pk];
+    return st;
+  };
+  auto normal = [&](int fi, double* nrm) {
+#pragma unroll
+    for (int c = 0; c < DIM; ++c)
+      nrm[c] = __ldg(M.tab.fv[DIR][c] + (int64_t)I[3 + c] * (N - 1) * N + (fi - 1) * N + line);
+  };
+  const double w = alpha * p.basis.inv_w[m];
+  const FaceState<DIM> own = state(m);
+  if (m >= 1) {  // interface fi = m: this node is its right node
+    double nrm[DIM], f[NV];
+    normal(m, nrm);
+    llf_flux<DIM>(state(m - 1), own, nrm, f);
+#pragma unroll
+    for (int q = 0; q < NV; ++q) acc[q] -= w * f[q];
+  }
+  if (m + 1 < N) {  // interface fi = m + 1: this node is its left node
+    double nrm[DIM], f[NV];
+    normal(m + 1, nrm);
+    llf_flux<DIM>(own, state(m + 1), nrm, f);
+#pragma unroll
+    for (int q = 0; q < NV; ++q) acc[q] += w * f[q];
+  }
+}
+
+template <int DIM, int N, int VF, int SF, int EPB, bool BATCH, bool HG>
 __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
-  using S = NodeShape<DIM, N, VF, EPB>;
+  static_assert(!HG || DIM == 2, "shock capturing: 2D only");
+  using S = NodeShape<DIM, N, VF, EPB, HG>;
   using K = NodeKernelSlots<DIM, VF>;
   constexpr int NV = S::NV, ND = S::ND, NDP = S::NDP, NF = S::NF, NFACE = S::NFACE,
                 NQ = S::NQ, NI = S::NI, NT = S::NT;
@@ -214,7 +269,9 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   double* us = smem_node;        // [el][var][pnode]
   double* pr = us + S::SM_U;     // [el][slot][pnode]
   double* sf = pr + S::SM_P;     // [el][face][fn][var]
-  int* info = reinterpret_cast<int*>(sf + S::SM_F);
+  double* alpha_s = sf + S::SM_F;          // [el] (shock capturing)
+  double* vinv_s = alpha_s + S::SM_A;      // [N][N] (shock capturing)
+  int* info = reinterpret_cast<int*>(vinv_s + S::SM_VINV);
   // [el][var][node] u_n tile (bulk-copy target; present when p.a != 0)
   double* stage_n = reinterpret_cast<double*>(reinterpret_cast<char*>(smem_node) + S::off_n_bytes);
 
@@ -288,6 +345,9 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
       I[6 + face] = nbr;
     }
   }
+  if constexpr (HG) {
+    for (int k = tid; k < N * N; k += NT) vinv_s[k] = p.basis.Vinv[k / N][k % N];
+  }
   {
     const double* src = M.u_in + (int64_t)e0 * NV * ND;
     for (int idx = tid; idx < ne * NV * ND; idx += NT) {
@@ -329,6 +389,47 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   }
   __syncthreads();
 
+  // ---- phase 1b: Hennemann-Gassner alpha per element (indicator.hpp:337-418),
+  // node-parallel with the same explicitly rounded arithmetic as
+  // stage_kernel.cuh (identical alpha and troubled-cell flags); scratch in the
+  // face buffer, which is written only afterwards ------------------------------
+  if constexpr (HG) {
+    double* ind = sf;                // [el][ND]
+    double* tmp = sf + EPB * ND;     // [el][ND]
+    double* m2 = sf + 2 * EPB * ND;  // [el][ND]
+    const int ii0 = node % N, jj0 = node / N;
+    if (active) {
+      const double* Ue = us + el * NV * NDP;
+      ind[el * ND + node] = hg_node_value(Ue[pn], Ue[NDP + pn], Ue[2 * NDP + pn], Ue[3 * NDP + pn]);
+    }
+    __syncthreads();
+    if (active) {
+      double r = 0.0;
+#pragma unroll
+      for (int ii = 0; ii < N; ++ii)
+        r = __dadd_rn(r, __dmul_rn(vinv_s[ii0 * N + ii], ind[el * ND + jj0 * N + ii]));
+      tmp[el * ND + node] = r;
+    }
+    __syncthreads();
+    if (active) {
+      double r = 0.0;
+#pragma unroll
+      for (int jj = 0; jj < N; ++jj)
+        r = __dadd_rn(r, __dmul_rn(vinv_s[jj0 * N + jj], tmp[el * ND + jj * N + ii0]));
+      m2[el * ND + node] = __dmul_rn(r, r);
+    }
+    __syncthreads();
+    if (tid < ne) {
+      double total, c1e, c2e;
+      hg_energy_sums<N>(m2 + tid * ND, &total, &c1e, &c2e);
+      const double a = hg_alpha_from_energies(total, c1e, c2e, p.hg_threshold, p.hg_s,
+                                              p.alpha_min, p.alpha_max);
+      alpha_s[tid] = a;
+      if (p.alpha_out) p.alpha_out[e0 + tid] = a;
+    }
+    __syncthreads();
+  }
+
   // ---- phase 2a: face fluxes, one task per (element, face, face node) ------
   for (int idx = tid; idx < ne * NFACE * NF; idx += NT) {
     const int fe = idx / (NFACE * NF);
@@ -369,6 +470,17 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
     node_volume_direction<1, DIM, N, VF, NDP>(p, M, U, P, I, node, pn, own, hgm1, acc);
     if constexpr (DIM == 3)
       node_volume_direction<2, DIM, N, VF, NDP>(p, M, U, P, I, node, pn, own, hgm1, acc);
+    if constexpr (HG) {
+      // volume_flux.hpp:817-842: (1 - alpha) DG + alpha FV for troubled elements
+      const double alpha = alpha_s[el];
+      if (fabs(alpha - 0.0) > p.atol) {
+        const double one_m = 1.0 - alpha;
+#pragma unroll
+        for (int q = 0; q < NV; ++q) acc[q] *= one_m;
+        node_fv_direction<0, DIM, N, VF, NDP>(p, M, U, P, I, node, alpha, acc);
+        node_fv_direction<1, DIM, N, VF, NDP>(p, M, U, P, I, node, alpha, acc);
+      }
+    }
   }
   __syncthreads();
   // the block agrees on a timeout (vote) so that all of it leaves together
@@ -415,17 +527,17 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   if (bad) atomicOr(p.nonfinite, 1u);
 }
 
-template <int DIM, int N, int VF, int SF, int EPB, bool BATCH>
+template <int DIM, int N, int VF, int SF, int EPB, bool BATCH, bool HG = false>
 __global__ void __launch_bounds__(EPB* ipow(N, DIM)) stage_node_kernel(const StageArgs<N> p) {
-  stage_node_body<DIM, N, VF, SF, EPB, BATCH>(p);
+  stage_node_body<DIM, N, VF, SF, EPB, BATCH, HG>(p);
 }
 
 // Same kernel with MINB resident blocks per SM requested from the register
 // allocator.
-template <int DIM, int N, int VF, int SF, int EPB, bool BATCH, int MINB>
+template <int DIM, int N, int VF, int SF, int EPB, bool BATCH, int MINB, bool HG = false>
 __global__ void __launch_bounds__(EPB* ipow(N, DIM), MINB)
     stage_node_kernel_capped(const StageArgs<N> p) {
-  stage_node_body<DIM, N, VF, SF, EPB, BATCH>(p);
+  stage_node_body<DIM, N, VF, SF, EPB, BATCH, HG>(p);
 }
 
 }  // namespace dgsem

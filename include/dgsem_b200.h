@@ -269,11 +269,12 @@ dgsem_status dgsem_check_finite(dgsem_ctx* ctx);
 /* Launch-shape autotuner (no reference counterpart; the reference has one
  * fixed Kokkos launch shape).  The fused stage kernel has up to 6 launch
  * shapes: 0-2 line-parallel (elements per block, register cap; bitwise
- * identical results), 3-4 node-parallel with and without a register cap, 5
+ * identical results), 3-4 node-parallel with and without a register cap
+ * (split form with or without shock capturing, not Navier-Stokes), 5
  * persistent node-parallel streaming element tiles through shared memory
- * with bulk copies (3-5: split form without shock capturing or viscous
- * terms; 5: 2D or even n in 3D; same results as 3; 3-5 agree with 0-2 to
- * rounding: same fluxes, different summation order).  dgsem_autotune times
+ * with bulk copies (no shock capturing; 2D or even n in 3D; same results as
+ * 3); 3-5 agree with 0-2 to rounding (same fluxes and the same alpha and
+ * troubled-cell flags, different summation order).  dgsem_autotune times
  * one SSPRK3 step from state u (into the context temporaries; u is not
  * modified) with each available shape, keeps the fastest and returns it in
  * *chosen (may be NULL); times_ms (6 doubles, may be NULL; 0 for an

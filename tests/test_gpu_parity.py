@@ -312,30 +312,35 @@ def test_launch_variants(name, cuda):
     torch.cuda.synchronize()
     for v in (1, 2):
         assert torch.equal(outs[0], outs[v]), v
-    node_variant = not (case.get("shock_capturing") or case.get("viscous"))
+    # node-parallel shapes 3-4 (also with shock capturing) and the persistent
+    # shape 5 (no shock capturing): same arithmetic per flux, different
+    # summation order; 3, 4 and 5 give the same bits
+    node_variant = not case.get("viscous")
+    pipe_variant = node_variant and not case.get("shock_capturing")
     if node_variant:
-        # node-parallel shapes: same arithmetic per flux, different summation
-        # order (each pair evaluated by both of its nodes); 3 and 4 differ
-        # only in the register cap and give the same bits
         node_outs = []
-        for v in (3, 4, 5):
+        for v in ((3, 4, 5) if pipe_variant else (3, 4)):
             solver.set_launch_variant(v)
             du3 = torch.empty_like(u)
             solver.rhs(u, du3, 0.05)
             node_outs.append(du3)
         torch.cuda.synchronize()
-        assert torch.equal(node_outs[0], node_outs[1])
-        assert torch.equal(node_outs[0], node_outs[2])
+        for other in node_outs[1:]:
+            assert torch.equal(node_outs[0], other)
         a, b = node_outs[0].cpu().numpy(), outs[0].cpu().numpy()
         assert rel_linf(a, b) <= RTOL
         assert rel_linf(dev_to_ref(a, solver.mesh.n_cells), do.rhs(s, u_ref, 0.05)) <= RTOL
     else:
         with pytest.raises(Exception):
             solver.set_launch_variant(3)
+    if not pipe_variant:
+        with pytest.raises(Exception):
+            solver.set_launch_variant(5)
+    nvar = 6 if pipe_variant else 5 if node_variant else 3
     chosen, times = solver.autotune(u, retime=True)
     torch.cuda.synchronize()
-    assert chosen in ((0, 1, 2, 3, 4, 5) if node_variant else (0, 1, 2))
-    assert all(t > 0.0 for t in times[:5 if node_variant else 3])
+    assert chosen in range(nvar)
+    assert all(t > 0.0 for t in times[:nvar])
     assert torch.equal(u, u_copy)
     du = torch.empty_like(u)
     solver.rhs(u, du, 0.05)
@@ -373,3 +378,21 @@ def test_node_parallel_variant_dmr_boundaries(cuda):
     solver.set_launch_variant(3)
     du_d = device_rhs(solver, u, t, cuda)
     assert rel_linf(du_d, du_o) <= RTOL, rel_linf(du_d, du_o)
+
+
+@pytest.mark.parametrize("name,sf", [("kh_hg", "llf"), ("kh_hg", "hllc"), ("dmr", "llf"),
+                                     ("dmr", "hllc")])
+def test_node_parallel_shock_capturing(name, sf, cuda):
+    """Node-parallel shapes with Hennemann-Gassner blending (same alpha and
+    flags as the line-parallel kernel: any flag flip would move the RHS by far
+    more than the bar) against the oracle, incl. the DMR boundary states."""
+    case = CASES[name]
+    s = make_oracle(case, "chandrashekar", sf)
+    u = initial(case, s, seed=5)
+    t = 0.02 if name == "dmr" else 0.0
+    du_o = do.rhs(s, u, t)
+    solver = make_device(case, "chandrashekar", sf)
+    for v in (3, 4):
+        solver.set_launch_variant(v)
+        du_d = device_rhs(solver, u, t, cuda)
+        assert rel_linf(du_d, du_o) <= RTOL, (v, rel_linf(du_d, du_o))
