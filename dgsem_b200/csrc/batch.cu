@@ -180,28 +180,41 @@ dgsem_status dgsem_batch_autotune(dgsem_batch* b, double* u, const double* dt_ho
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
+  // Rounds that each time every variant once, starting at a different
+  // variant per round; the group keeps the variant with the smallest median.
+  constexpr int rounds = 5;
   int gi = 0;
   for (Group& g : b->groups) {
+    const int nv = g.engine->num_variants();
+    std::vector<float> ms((size_t)rounds * nv, 0.f);
+    // stage 1 writes tmp1 only, so repeated launches leave u untouched
+    auto run = [&]() {
+      return g.engine->batch_stage(g.cfg, b->views, g.tile_mesh, g.tile_e0, g.ntiles, 0.0,
+                                   1.0, 0.0, nullptr, b->stream);
+    };
+    for (int r = 0; r < rounds && st == DGSEM_OK; ++r)
+      for (int k = 0; k < nv && st == DGSEM_OK; ++k) {
+        const int v = (r + k) % nv;
+        g.engine->set_variant(v);
+        if (build_tiles(b, g) != cudaSuccess || run() != cudaSuccess) {
+          st = DGSEM_ERR_CUDA;
+          break;
+        }
+        cudaEventRecord(e0, b->stream);
+        for (int q = 0; q < 3 && st == DGSEM_OK; ++q)
+          if (run() != cudaSuccess) st = DGSEM_ERR_CUDA;
+        cudaEventRecord(e1, b->stream);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms[(size_t)r * nv + v], e0, e1);
+      }
     int best = 0;
     float best_ms = 1e30f;
-    for (int v = 0; v < g.engine->num_variants() && st == DGSEM_OK; ++v) {
-      g.engine->set_variant(v);
-      if (build_tiles(b, g) != cudaSuccess) st = DGSEM_ERR_CUDA;
-      // stage 1 writes tmp1 only, so repeated launches leave u untouched
-      auto run = [&]() {
-        return g.engine->batch_stage(g.cfg, b->views, g.tile_mesh, g.tile_e0, g.ntiles, 0.0,
-                                     1.0, 0.0, nullptr, b->stream);
-      };
-      if (st == DGSEM_OK && run() != cudaSuccess) st = DGSEM_ERR_CUDA;
-      cudaEventRecord(e0, b->stream);
-      for (int r = 0; r < 3 && st == DGSEM_OK; ++r)
-        if (run() != cudaSuccess) st = DGSEM_ERR_CUDA;
-      cudaEventRecord(e1, b->stream);
-      cudaEventSynchronize(e1);
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, e0, e1);
-      if (ms < best_ms) {
-        best_ms = ms;
+    for (int v = 0; v < nv; ++v) {
+      float m[rounds];
+      for (int r = 0; r < rounds; ++r) m[r] = ms[(size_t)r * nv + v];
+      std::sort(m, m + rounds);
+      if (m[rounds / 2] < best_ms) {
+        best_ms = m[rounds / 2];
         best = v;
       }
     }

@@ -3,6 +3,7 @@
 // layout conversion).  The fused stage kernel lives in stage_kernel.cuh.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -688,42 +689,52 @@ std::string tune_key(int ndims, int n, int vf, int sf, int hg, int ns, int64_t n
 }
 
 // Times `launch` (one SSPRK3 step on `s`) for each variant of `eng`: one
-// warm-up, then `reps` timed launches, each preceded (outside the timed
-// region) by a write of `flush_bytes` to `flush` when given, which evicts L2
-// so that every timed step streams its states from HBM.  Returns the fastest
-// variant and optionally the mean times.
+// warm-up per variant, then `rounds` rounds that each time every variant once,
+// starting the round at a different variant so that no variant is always
+// timed first or always after the same neighbour (clock and power drift then
+// spreads over all variants instead of favouring one).  Each timed launch is
+// preceded (outside the timed region) by a write of `flush_bytes` to `flush`
+// when given, which evicts L2 so that every timed step streams its states
+// from HBM.  Returns the variant with the smallest median time and optionally
+// the medians.
 template <class Launch>
 int time_variants(EngineBase* eng, cudaStream_t s, Launch&& launch, double* times_ms,
                   void* flush, size_t flush_bytes) {
-  constexpr int reps = 5;
-  cudaEvent_t ev[2 * reps];
+  constexpr int rounds = 7;
+  const int nv = eng->num_variants();
+  std::vector<cudaEvent_t> ev(2 * rounds * nv);
   for (auto& e : ev) cudaEventCreate(&e);
+  for (int v = 0; v < nv; ++v) {
+    eng->set_variant(v);
+    launch();
+  }
+  for (int r = 0; r < rounds; ++r)
+    for (int k = 0; k < nv; ++k) {
+      const int v = (r + k) % nv;
+      eng->set_variant(v);
+      if (flush) cudaMemsetAsync(flush, (r * nv + k) & 0xff, flush_bytes, s);
+      cudaEventRecord(ev[2 * (r * nv + v)], s);
+      launch();
+      cudaEventRecord(ev[2 * (r * nv + v) + 1], s);
+    }
+  cudaStreamSynchronize(s);
   int best = 0;
   float best_ms = 1e30f;
   for (int v = 0; v < kNumVariants; ++v) {
-    if (v >= eng->num_variants()) {
+    if (v >= nv) {
       if (times_ms) times_ms[v] = 0.0;
       continue;
     }
-    eng->set_variant(v);
-    launch();  // warm-up
-    for (int r = 0; r < reps; ++r) {
-      if (flush) cudaMemsetAsync(flush, r & 0xff, flush_bytes, s);
-      cudaEventRecord(ev[2 * r], s);
-      launch();
-      cudaEventRecord(ev[2 * r + 1], s);
+    float ms[rounds];
+    for (int r = 0; r < rounds; ++r) {
+      ms[r] = 0.f;
+      cudaEventElapsedTime(&ms[r], ev[2 * (r * nv + v)], ev[2 * (r * nv + v) + 1]);
     }
-    cudaEventSynchronize(ev[2 * reps - 1]);
-    float ms = 0.f;
-    for (int r = 0; r < reps; ++r) {
-      float m = 0.f;
-      cudaEventElapsedTime(&m, ev[2 * r], ev[2 * r + 1]);
-      ms += m;
-    }
-    ms /= reps;
-    if (times_ms) times_ms[v] = ms;
-    if (ms < best_ms) {
-      best_ms = ms;
+    std::sort(ms, ms + rounds);
+    const float med = ms[rounds / 2];
+    if (times_ms) times_ms[v] = med;
+    if (med < best_ms) {
+      best_ms = med;
       best = v;
     }
   }

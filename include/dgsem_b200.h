@@ -276,9 +276,10 @@ dgsem_status dgsem_check_finite(dgsem_ctx* ctx);
  * 3); 3-5 agree with 0-2 to rounding (same fluxes and the same alpha and
  * troubled-cell flags, different summation order).  dgsem_autotune times
  * one SSPRK3 step from state u (into the context temporaries; u is not
- * modified) with each available shape, keeps the fastest and returns it in
- * *chosen (may be NULL); times_ms (6 doubles, may be NULL; 0 for an
- * unavailable shape) receives the mean step times and forces re-timing.
+ * modified) with each available shape, 7 times in rounds that visit the
+ * shapes in rotated order, keeps the one with the smallest median and returns
+ * it in *chosen (may be NULL); times_ms (6 doubles, may be NULL; 0 for an
+ * unavailable shape) receives the median step times and forces re-timing.
  * Every timed step is preceded by an L2 eviction (a 256 MiB temporary
  * buffer, freed before returning), i.e. states stream from HBM as in large
  * runs; with the environment variable DGSEM_AUTOTUNE_WARM set, steps are
