@@ -294,6 +294,30 @@ __device__ __forceinline__ constexpr int padn(int node) {
   return node + node / N;
 }
 
+// Copies the u tile [el][var][node] of `ne` elements from `src` (global) to
+// the padded shared layout `us`.  For a full tile (ne == EPB) each thread
+// issues all of its loads before its first store, so the block waits for one
+// global round trip instead of one per loop iteration.
+template <int N, int NV, int ND, int NDP, int EPB, int NT>
+__device__ __forceinline__ void load_element_tile(const double* src, double* us, int ne,
+                                                  int tid) {
+  constexpr int TILE = EPB * NV * ND, PER = (TILE + NT - 1) / NT;
+  if (ne == EPB) {
+    double v[PER];
+#pragma unroll
+    for (int r = 0; r < PER; ++r)
+      if (TILE % NT == 0 || tid + r * NT < TILE) v[r] = __ldg(src + tid + r * NT);
+#pragma unroll
+    for (int r = 0; r < PER; ++r) {
+      const int idx = tid + r * NT;
+      if (TILE % NT == 0 || idx < TILE) us[(idx / ND) * NDP + padn<N>(idx % ND)] = v[r];
+    }
+  } else {
+    for (int idx = tid; idx < ne * NV * ND; idx += NT)
+      us[(idx / ND) * NDP + padn<N>(idx % ND)] = __ldg(src + idx);
+  }
+}
+
 // Per-node shared-memory slots: the velocity, the flux-specific scalars and
 // -1/J.  Chandrashekar needs (p, beta, kin), Ranocha (p), Kennedy-Gruber
 // (p, e); p is always present because the surface fluxes use it.
@@ -716,13 +740,7 @@ __device__ __forceinline__ void stage_body(const StageArgs<N>& p) {
   if (HG) {
     for (int k = tid; k < N * N; k += NT) vinv_s[k] = p.basis.Vinv[k / N][k % N];
   }
-  {
-    const double* src = M.u_in + (int64_t)e0 * NV * ND;
-    for (int idx = tid; idx < ne * NV * ND; idx += NT) {
-      const int row = idx / ND, node = idx % ND;
-      us[row * NDP + padn<N>(node)] = __ldg(src + idx);
-    }
-  }
+  load_element_tile<N, NV, ND, NDP, EPB, NT>(M.u_in + (int64_t)e0 * NV * ND, us, ne, tid);
   __syncthreads();
 
   // ---- phase 1: node primitives, -1/J, HG alpha, -F_v -----------------

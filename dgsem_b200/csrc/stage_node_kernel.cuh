@@ -348,13 +348,7 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   if constexpr (HG) {
     for (int k = tid; k < N * N; k += NT) vinv_s[k] = p.basis.Vinv[k / N][k % N];
   }
-  {
-    const double* src = M.u_in + (int64_t)e0 * NV * ND;
-    for (int idx = tid; idx < ne * NV * ND; idx += NT) {
-      const int row = idx / ND, node = idx % ND;
-      us[row * NDP + padn<N>(node)] = __ldg(src + idx);
-    }
-  }
+  load_element_tile<N, NV, ND, NDP, EPB, NT>(M.u_in + (int64_t)e0 * NV * ND, us, ne, tid);
   __syncthreads();
 
   // ---- phase 1: node data, sound speed and -1/J --------------------------
