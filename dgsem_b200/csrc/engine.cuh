@@ -10,6 +10,7 @@
 #include <stdint.h>
 
 #include <memory>
+#include <utility>
 
 #include "br1_kernel.cuh"
 #include "stage_kernel.cuh"
@@ -118,6 +119,28 @@ struct NodeLaunch {
   static constexpr int MINB = 65536 / (NT * 72) > 1 ? 65536 / (NT * 72) : 1;
 };
 
+// Launches a stage kernel with programmatic stream serialization: the GPU
+// may schedule its blocks while the previous kernel on `s` drains (hiding the
+// launch gap between the three stages of a step); the kernel's first
+// instruction, griddepcontrol.wait (stage_dependency_sync), holds every block
+// until that kernel has completed and flushed its writes.  After a copy, a
+// memset or an event the launch is ordered as usual.
+template <class... P, class... A>
+void launch_stage_kernel(void (*kernel)(P...), unsigned grid, unsigned block, size_t smem,
+                         cudaStream_t s, A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
+
 template <int DIM, int N, int VF, int SF, bool HG, bool NS = false>
 class Engine final : public EngineBase {
  public:
@@ -173,13 +196,15 @@ class Engine final : public EngineBase {
   void launch_node(const StageArgs<N>& args, int64_t nelem, cudaStream_t s) const {
     if constexpr (kNode) {
       const int64_t blocks = (nelem + NL::EPB - 1) / NL::EPB;
-      node_kernel<false, CAP>()<<<(unsigned)blocks, NL::NT, node_smem(args), s>>>(args);
+      launch_stage_kernel(node_kernel<false, CAP>(), (unsigned)blocks, NL::NT, node_smem(args), s,
+                          args);
     }
   }
   template <bool CAP>
   void launch_node_batch(const StageArgs<N>& args, int ntiles, cudaStream_t s) const {
     if constexpr (kBatch)
-      node_kernel<true, CAP>()<<<(unsigned)ntiles, NL::NT, node_smem(args), s>>>(args);
+      launch_stage_kernel(node_kernel<true, CAP>(), (unsigned)ntiles, NL::NT, node_smem(args), s,
+                          args);
   }
 
   using PSh = PipeShape<DIM, N, VF, NL::EPB>;
@@ -208,7 +233,8 @@ class Engine final : public EngineBase {
       }
       const int64_t ntiles = (nelem + NL::EPB - 1) / NL::EPB;
       const int64_t blocks = ntiles < pipe_blocks_ ? ntiles : pipe_blocks_;
-      pipe_kernel()<<<(unsigned)blocks, PSh::NT, PSh::smem_bytes, s>>>(args, (int)ntiles);
+      launch_stage_kernel(pipe_kernel(), (unsigned)blocks, PSh::NT, PSh::smem_bytes, s, args,
+                          (int)ntiles);
     } else {
       launch_node<true>(args, nelem, s);
     }
@@ -261,7 +287,7 @@ class Engine final : public EngineBase {
   void launch(const StageArgs<N>& args, int64_t nelem, cudaStream_t s) const {
     using L = LaunchShape<DIM, N, V>;
     const int64_t blocks = (nelem + L::EPB - 1) / L::EPB;
-    kernel<V>()<<<(unsigned)blocks, L::NT, Sh<V>::smem_bytes, s>>>(args);
+    launch_stage_kernel(kernel<V>(), (unsigned)blocks, L::NT, Sh<V>::smem_bytes, s, args);
   }
 
   cudaError_t stage(const EngineConfig& cfg, const double* u_n,
@@ -307,7 +333,7 @@ class Engine final : public EngineBase {
   void launch_batch(const StageArgs<N>& args, int ntiles, cudaStream_t s) const {
     if constexpr (kBatch) {
       using L = LaunchShape<DIM, N, V>;
-      batch_kernel<V>()<<<(unsigned)ntiles, L::NT, Sh<V>::smem_bytes, s>>>(args);
+      launch_stage_kernel(batch_kernel<V>(), (unsigned)ntiles, L::NT, Sh<V>::smem_bytes, s, args);
     }
   }
 

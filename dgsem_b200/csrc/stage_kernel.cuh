@@ -294,6 +294,17 @@ __device__ __forceinline__ constexpr int padn(int node) {
   return node + node / N;
 }
 
+// Programmatic dependent launch: the stage kernels are launched with
+// programmatic stream serialization, so a stage kernel may be scheduled while
+// the previous kernel on its stream is still draining.  Each block first
+// waits for that kernel's completion and memory flush (before it reads any
+// kernel argument array), then lets the next kernel be scheduled.  Both
+// instructions are no-ops in a normal launch.
+__device__ __forceinline__ void stage_dependency_sync() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Copies the u tile [el][var][node] of `ne` elements from `src` (global) to
 // the padded shared layout `us`.  For a full tile (ne == EPB) each thread
 // issues all of its loads before its first store, so the block waits for one
@@ -678,6 +689,7 @@ __device__ __forceinline__ void stage_body(const StageArgs<N>& p) {
   double* vinv_s = wv + S::SM_W;     // inverse Legendre Vandermonde (HG)
   int* info = reinterpret_cast<int*>(vinv_s + S::SM_VINV);
 
+  stage_dependency_sync();
   const int tid = threadIdx.x;
   // Batched launches stage the block's mesh view in shared memory; single-mesh
   // launches read it from the kernel parameters (constant bank), which keeps

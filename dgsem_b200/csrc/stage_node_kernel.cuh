@@ -275,6 +275,7 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   // [el][var][node] u_n tile (bulk-copy target; present when p.a != 0)
   double* stage_n = reinterpret_cast<double*>(reinterpret_cast<char*>(smem_node) + S::off_n_bytes);
 
+  stage_dependency_sync();
   const int tid = threadIdx.x;
   __shared__ MeshView mesh_s;
   int e0;

@@ -55,6 +55,7 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
   int* info = reinterpret_cast<int*>(sf + S::B::SM_F);
   __shared__ uint64_t bar_in, bar_n;
 
+  stage_dependency_sync();
   const MeshView& M = p.mesh;
   const int tid = threadIdx.x;
   const int nelem = M.nelem;
