@@ -286,12 +286,14 @@ __device__ double hg_alpha_2d(const double* us_el, int ND, const BasisConst<N>& 
 // ---------------------------------------------------------------------------
 // The fused stage kernel
 // ---------------------------------------------------------------------------
-// Shared-memory node arrays are padded by one slot per N nodes
-// (pnode = node + node / N) so that the per-line strided accesses of the
-// volume phase fall on distinct banks.
-template <int N>
+// Shared-memory node arrays of the line-parallel kernel are padded by one
+// slot per N nodes (pnode = node + node / N) so that the per-line strided
+// accesses of the volume phase fall on distinct banks.  The node-parallel
+// kernels, whose warps read 32 consecutive nodes shifted along one line,
+// use the unpadded layout (PAD = false).
+template <int N, bool PAD = true>
 __device__ __forceinline__ constexpr int padn(int node) {
-  return node + node / N;
+  return PAD ? node + node / N : node;
 }
 
 // Programmatic dependent launch: the stage kernels are launched with
@@ -313,6 +315,7 @@ template <int N, int NV, int ND, int NDP, int EPB, int NT>
 __device__ __forceinline__ void load_element_tile(const double* src, double* us, int ne,
                                                   int tid) {
   constexpr int TILE = EPB * NV * ND, PER = (TILE + NT - 1) / NT;
+  constexpr bool PAD = NDP != ND;
   if (ne == EPB) {
     double v[PER];
 #pragma unroll
@@ -321,11 +324,11 @@ __device__ __forceinline__ void load_element_tile(const double* src, double* us,
 #pragma unroll
     for (int r = 0; r < PER; ++r) {
       const int idx = tid + r * NT;
-      if (TILE % NT == 0 || idx < TILE) us[(idx / ND) * NDP + padn<N>(idx % ND)] = v[r];
+      if (TILE % NT == 0 || idx < TILE) us[(idx / ND) * NDP + padn<N, PAD>(idx % ND)] = v[r];
     }
   } else {
     for (int idx = tid; idx < ne * NV * ND; idx += NT)
-      us[(idx / ND) * NDP + padn<N>(idx % ND)] = __ldg(src + idx);
+      us[(idx / ND) * NDP + padn<N, PAD>(idx % ND)] = __ldg(src + idx);
   }
 }
 
@@ -394,8 +397,9 @@ __device__ __forceinline__ void element_face_flux_state(
     const double* wv_el, const int* I, int dir, int side, int line, double gamma,
     double t_stage, int c0, int c1, int c2, double* f) {
   constexpr int NV = DIM + 2, ND = ipow(N, DIM);
+  constexpr bool PAD = NDP != ND;
   const int own_node = line_node<DIM, N>(dir, line, side ? N - 1 : 0);
-  const int opn = padn<N>(own_node);
+  const int opn = padn<N, PAD>(own_node);
   const int face = 2 * dir + side;
   const int en = I[6 + face];
   if (en >= 0) {
@@ -468,7 +472,8 @@ __device__ __forceinline__ void element_face_flux_state(
       for (int q = 0; q < NV; ++q) {
         double acc = 0.0;
 #pragma unroll
-        for (int m = 0; m < N; ++m) acc += us_el[q * NDP + padn<N>(line_node<DIM, N>(dir, line, m))];
+        for (int m = 0; m < N; ++m)
+          acc += us_el[q * NDP + padn<N, PAD>(line_node<DIM, N>(dir, line, m))];
         ub[q] = acc / (double)N;
       }
     } else if (kind == BC_MIXED_DMR_WALL && x < 1.0 / 6.0) {

@@ -57,7 +57,8 @@ template <int DIM, int N, int VF, int EPB, bool HG = false>
 struct NodeShape {
   static constexpr int NV = DIM + 2;
   static constexpr int ND = ipow(N, DIM);
-  static constexpr int NDP = ND + ND / N;
+  static constexpr bool PAD = false;  // unpadded node arrays (see padn)
+  static constexpr int NDP = PAD ? ND + ND / N : ND;
   static constexpr int NF = ipow(N, DIM - 1);
   static constexpr int NFACE = 2 * DIM;
   static constexpr int NQ = NodeKernelSlots<DIM, VF>::NQ;
@@ -177,9 +178,9 @@ __device__ __forceinline__ void node_volume_direction(const StageArgs<N>& p, con
                                                       double hgm1, double* acc) {
   constexpr int NV = DIM + 2, ND = ipow(N, DIM);
   constexpr bool HALF = NodeKernelSlots<DIM, VF>::HALF;
-  // node-index and padded-index strides along DIR
+  // node-index and shared-memory-index strides along DIR
   constexpr int SN = DIR == 0 ? 1 : DIR == 1 ? N : N * N;
-  constexpr int SP = DIR == 0 ? 1 : DIR == 1 ? N + 1 : N * N + N;
+  constexpr int SP = NDP == ND ? SN : DIR == 0 ? 1 : DIR == 1 ? N + 1 : N * N + N;
   const int m = DIR == 0 ? node % N : DIR == 1 ? (node / N) % N : node / (N * N);
   const double* jrow[DIM];
   double hja_own[DIM];
@@ -224,7 +225,7 @@ __device__ __forceinline__ void node_fv_direction(const StageArgs<N>& p, const M
   const int m = DIR == 0 ? node % N : node / N;
   const int line = DIR == 0 ? node / N : node % N;
   auto state = [&](int k) {
-    const int pk = padn<N>(line_node<DIM, N>(DIR, line, k));
+    const int pk = padn<N, (NDP != ipow(N, DIM))>(line_node<DIM, N>(DIR, line, k));
     FaceState<DIM> st;
 #pragma unroll
     for (int q = 0; q < NV; ++q) st.u[q] = U[q * NDP + pk];
@@ -355,7 +356,7 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   // ---- phase 1: node data, sound speed and -1/J --------------------------
   const int el = tid / ND, node = tid % ND;
   const bool active = el < ne;
-  const int pn = padn<N>(node);
+  const int pn = padn<N, S::PAD>(node);
   if (active) {
     double u[NV];
 #pragma unroll
@@ -434,7 +435,7 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
     const int* I = info + fe * NI;
     const double* U = us + fe * NV * NDP;
     const double* P = pr + fe * NQ * NDP;
-    const int opn = padn<N>(line_node<DIM, N>(dir, fn, side ? N - 1 : 0));
+    const int opn = padn<N, S::PAD>(line_node<DIM, N>(dir, fn, side ? N - 1 : 0));
     FaceState<DIM> so;
 #pragma unroll
     for (int q = 0; q < NV; ++q) so.u[q] = U[q * NDP + opn];

@@ -86,7 +86,7 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
   }
 
   const int el = tid / ND, node = tid % ND;
-  const int pn = padn<N>(node);
+  const int pn = padn<N, S::B::PAD>(node);
   uint32_t phase = 0;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x, phase ^= 1u) {
     const int e0 = t * EPB;
@@ -182,7 +182,7 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
       const int* I = info + fe * NI;
       const double* U = us + fe * NV * NDP;
       const double* P = pr + fe * NQ * NDP;
-      const int opn = padn<N>(line_node<DIM, N>(dir, fn, side ? N - 1 : 0));
+      const int opn = padn<N, S::B::PAD>(line_node<DIM, N>(dir, fn, side ? N - 1 : 0));
       FaceState<DIM> so;
 #pragma unroll
       for (int q = 0; q < NV; ++q) so.u[q] = U[q * NDP + opn];
