@@ -4,11 +4,12 @@
 // occupancy instead of minimal flux count.
 //
 // Per block: EPB elements, EPB * n^d threads.
-//   0  element info and the coalesced u_in tile (padded shared memory);
+//   0  element info and the coalesced u_in tile (unpadded shared memory);
 //   1  per-node flux data (NodeKernelSlots), sound speed and -1/J;
 //   2a face tasks: every (face, face node) of the block's elements computes
 //      its interface / boundary flux f* once into a shared face buffer
-//      (faces of one direction are consecutive, so warps stay uniform);
+//      (tasks ordered side-major, so a warp's lanes share the face side and
+//      evaluate the flux in one argument order);
 //   2b one thread per node: for each direction, the two-point fluxes with the
 //      n-1 other nodes of its line, sum_k Dsplit(m, k) f(u_m, u_k, (Ja_m +
 //      Ja_k)/2), accumulated in registers (each pair is evaluated by both of
@@ -428,10 +429,14 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
 
   // ---- phase 2a: face fluxes, one task per (element, face, face node) ------
   for (int idx = tid; idx < ne * NFACE * NF; idx += NT) {
-    const int fe = idx / (NFACE * NF);
-    const int face = (idx / NF) % NFACE;
-    const int fn = idx % NF;
-    const int dir = face >> 1, side = face & 1;
+    // side-major task order: the lanes of a warp share the face side, so
+    // they take one branch of the (own, neighbour) flux ordering
+    const int side = idx >= ne * DIM * NF ? 1 : 0;
+    const int r = idx - side * ne * DIM * NF;
+    const int fe = r / (DIM * NF);
+    const int dir = (r / NF) % DIM;
+    const int fn = r % NF;
+    const int face = 2 * dir + side;
     const int* I = info + fe * NI;
     const double* U = us + fe * NV * NDP;
     const double* P = pr + fe * NQ * NDP;

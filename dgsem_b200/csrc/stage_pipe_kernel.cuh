@@ -175,10 +175,14 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
 
     // ---- phase 2a: face fluxes ---------------------------------------------
     for (int idx = tid; idx < ne * NFACE * NF; idx += NT) {
-      const int fe = idx / (NFACE * NF);
-      const int face = (idx / NF) % NFACE;
-      const int fn = idx % NF;
-      const int dir = face >> 1, side = face & 1;
+      // side-major task order: the lanes of a warp share the face side, so
+      // they take one branch of the (own, neighbour) flux ordering
+      const int side = idx >= ne * DIM * NF ? 1 : 0;
+      const int r = idx - side * ne * DIM * NF;
+      const int fe = r / (DIM * NF);
+      const int dir = (r / NF) % DIM;
+      const int fn = r % NF;
+      const int face = 2 * dir + side;
       const int* I = info + fe * NI;
       const double* U = us + fe * NV * NDP;
       const double* P = pr + fe * NQ * NDP;
