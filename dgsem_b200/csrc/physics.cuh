@@ -173,6 +173,28 @@ struct FaceState {
   double a;  // sound speed
 };
 
+// (L, R) = first ? (a, b) : (b, a), field by field with selects, so that
+// one flux evaluation serves both argument orders.
+template <int DIM>
+__device__ __forceinline__ void order_states(bool first, const FaceState<DIM>& a,
+                                             const FaceState<DIM>& b, FaceState<DIM>& L,
+                                             FaceState<DIM>& R) {
+#pragma unroll
+  for (int q = 0; q < DIM + 2; ++q) {
+    L.u[q] = first ? a.u[q] : b.u[q];
+    R.u[q] = first ? b.u[q] : a.u[q];
+  }
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    L.v[d] = first ? a.v[d] : b.v[d];
+    R.v[d] = first ? b.v[d] : a.v[d];
+  }
+  L.p = first ? a.p : b.p;
+  R.p = first ? b.p : a.p;
+  L.a = first ? a.a : b.a;
+  R.a = first ? b.a : a.a;
+}
+
 template <int DIM>
 __device__ __forceinline__ FaceState<DIM> prepare_face(const double* u,
                                                        double gamma) {

@@ -402,36 +402,70 @@ __device__ __forceinline__ void element_face_flux_state(
   const int opn = padn<N, PAD>(own_node);
   const int face = 2 * dir + side;
   const int en = I[6 + face];
+  // the state on the far side of the face (neighbour trace or boundary
+  // state) and the face normal; one flux evaluation follows for both cases
+  double ux[NV], nrm[DIM];
+  const int nb_node = line_node<DIM, N>(dir, line, side ? 0 : N - 1);
   if (en >= 0) {
-    const int nb_node = line_node<DIM, N>(dir, line, side ? 0 : N - 1);
-    double un[NV];
 #pragma unroll
-    for (int q = 0; q < NV; ++q) un[q] = __ldg(M.u_in + ((int64_t)en * NV + q) * ND + nb_node);
-    const FaceState<DIM> sn = prepare_face<DIM>(un, gamma);
+    for (int q = 0; q < NV; ++q) ux[q] = __ldg(M.u_in + ((int64_t)en * NV + q) * ND + nb_node);
     // normal: Ja^dir of the element on the high side at its low-face node
     const int r_node = line_node<DIM, N>(dir, line, 0);
     const int cells[3] = {c0, c1, c2};
     int npos = I[dir] + 1;
     if (npos >= cells[dir]) npos = 0;
-    double nrm[DIM];
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
       const int eo = side ? eidx_other_shift<DIM>(I, c, dir, npos, c0, c1) : I[3 + c];
       nrm[c] = ja_at(M.tab.ja[dir][c], eo, ND, r_node);
     }
-    if (side) {
-      surface_flux<DIM, SF>(so, sn, nrm, gamma, f);
-    } else {
-      surface_flux<DIM, SF>(sn, so, nrm, gamma, f);
+  } else {
+    // boundary face (boundary_helper.hpp:93-146): own metric at the boundary
+    // node; the inner state is the left state on high faces.
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) nrm[c] = ja_at(M.tab.ja[dir][c], I[3 + c], ND, own_node);
+    const int kind = p.bc.kind[face];
+    if (DIM == 2) {
+      const double x = __ldg(M.tab.coord[0] + I[0] * N + (own_node % N));
+      const double y = __ldg(M.tab.coord[1] + I[1] * N + (own_node / N));
+      if (kind == BC_DIRICHLET_DMR || (kind == BC_MIXED_DMR_WALL && x < 1.0 / 6.0)) {
+        dmr_state(p.bc, x, y, t_stage, ux);
+      } else if (kind == BC_DIRICHLET_CONST) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) ux[q] = p.bc.state[q];
+      } else if (kind == BC_OUTFLOW) {
+        // outflow_boundary.hpp:79-104: average along the line normal to the face
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+          double acc = 0.0;
+#pragma unroll
+          for (int m = 0; m < N; ++m)
+            acc += us_el[q * NDP + padn<N, PAD>(line_node<DIM, N>(dir, line, m))];
+          ux[q] = acc / (double)N;
+        }
+      } else {  // slip wall / wall branch of the mixed BC
+        reflect_state(so.u, nrm, ux);
+      }
+    } else {  // 3D meshes are periodic: no boundary faces
+#pragma unroll
+      for (int q = 0; q < NV; ++q) ux[q] = so.u[q];
     }
-    if constexpr (NS) {
+  }
+  const FaceState<DIM> sx = prepare_face<DIM>(ux, gamma);
+  if (side) {
+    surface_flux<DIM, SF>(so, sx, nrm, gamma, f);
+  } else {
+    surface_flux<DIM, SF>(sx, so, nrm, gamma, f);
+  }
+  if constexpr (NS) {
+    if (en >= 0) {
       // one-sided viscous interface flux: -F_v . n of the high-side (primary)
       // element at its low-face node (parabolic_viscous.hpp:570-585), lifted
       // with the same factors as the inviscid flux
       double w[2][4];
       if (side) {
         double q[4], gx[4], gy[4];
-        ns_gradient_variables(un, gamma, q);
+        ns_gradient_variables(ux, gamma, q);
         const double* G = p.grad + (int64_t)en * 4 * 2 * ND + nb_node;
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
@@ -449,44 +483,6 @@ __device__ __forceinline__ void element_face_flux_state(
 #pragma unroll
       for (int v = 0; v < 4; ++v) f[v] += w[0][v] * nrm[0] + w[1][v] * nrm[1];
     }
-    return;
-  }
-  // boundary face (boundary_helper.hpp:93-146): own metric at the boundary
-  // node; the inner state is the left state on high faces.
-  double nrm[DIM];
-#pragma unroll
-  for (int c = 0; c < DIM; ++c) nrm[c] = ja_at(M.tab.ja[dir][c], I[3 + c], ND, own_node);
-  double ub[NV];
-  const int kind = p.bc.kind[face];
-  if (DIM == 2) {
-    const double x = __ldg(M.tab.coord[0] + I[0] * N + (own_node % N));
-    const double y = __ldg(M.tab.coord[1] + I[1] * N + (own_node / N));
-    if (kind == BC_DIRICHLET_DMR) {
-      dmr_state(p.bc, x, y, t_stage, ub);
-    } else if (kind == BC_DIRICHLET_CONST) {
-#pragma unroll
-      for (int q = 0; q < NV; ++q) ub[q] = p.bc.state[q];
-    } else if (kind == BC_OUTFLOW) {
-      // outflow_boundary.hpp:79-104: average along the line normal to the face
-#pragma unroll
-      for (int q = 0; q < NV; ++q) {
-        double acc = 0.0;
-#pragma unroll
-        for (int m = 0; m < N; ++m)
-          acc += us_el[q * NDP + padn<N, PAD>(line_node<DIM, N>(dir, line, m))];
-        ub[q] = acc / (double)N;
-      }
-    } else if (kind == BC_MIXED_DMR_WALL && x < 1.0 / 6.0) {
-      dmr_state(p.bc, x, y, t_stage, ub);
-    } else {  // slip wall / wall branch of the mixed BC
-      reflect_state(so.u, nrm, ub);
-    }
-  }
-  const FaceState<DIM> sb = prepare_face<DIM>(ub, gamma);
-  if (side) {
-    surface_flux<DIM, SF>(so, sb, nrm, gamma, f);
-  } else {
-    surface_flux<DIM, SF>(sb, so, nrm, gamma, f);
   }
 }
 

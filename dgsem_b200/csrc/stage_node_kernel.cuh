@@ -244,19 +244,22 @@ __device__ __forceinline__ void node_fv_direction(const StageArgs<N>& p, const M
   };
   const double w = alpha * p.basis.inv_w[m];
   const FaceState<DIM> own = state(m);
-  if (m >= 1) {  // interface fi = m: this node is its right node
+  // s = 0: interface fi = m, this node is its right node (-w f);
+  // s = 1: interface fi = m + 1, this node is its left node (+w f).
+  // One flux evaluation site keeps the kernel's code small.
+#pragma unroll 1
+  for (int s = 0; s < 2; ++s) {
+    const int fi = m + s;
+    if (fi < 1 || fi > N - 1) continue;
     double nrm[DIM], f[NV];
-    normal(m, nrm);
-    llf_flux<DIM>(state(m - 1), own, nrm, f);
+    normal(fi, nrm);
+    const FaceState<DIM> other = state(s ? m + 1 : m - 1);
+    FaceState<DIM> L, R;
+    order_states<DIM>(s != 0, own, other, L, R);
+    llf_flux<DIM>(L, R, nrm, f);
+    const double ws = s ? w : -w;
 #pragma unroll
-    for (int q = 0; q < NV; ++q) acc[q] -= w * f[q];
-  }
-  if (m + 1 < N) {  // interface fi = m + 1: this node is its left node
-    double nrm[DIM], f[NV];
-    normal(m + 1, nrm);
-    llf_flux<DIM>(own, state(m + 1), nrm, f);
-#pragma unroll
-    for (int q = 0; q < NV; ++q) acc[q] += w * f[q];
+    for (int q = 0; q < NV; ++q) acc[q] += ws * f[q];
   }
 }
 
