@@ -170,8 +170,13 @@ __device__ __forceinline__ void node_volume_flux(const NodeFluxState<DIM>& L,
 }
 
 // Volume contribution of direction DIR to the node at padded position `pn`,
-// node index `node`, position m on its line.
-template <int DIR, int DIM, int N, int VF, int NDP>
+// node index `node`, position m on its line.  WARP_ALL: every lane of the
+// calling warp executes the call (thread = element * n^d + node, blocks a
+// multiple of 32 threads); then, where a whole line of direction DIR lies in
+// one warp, the partners' metric terms come from the partners' lanes by
+// shuffle instead of a second global load (the same values, so the same
+// normal bit for bit).
+template <int DIR, int DIM, int N, int VF, int NDP, bool WARP_ALL = false>
 __device__ __forceinline__ void node_volume_direction(const StageArgs<N>& p, const MeshView& M,
                                                       const double* U, const double* P,
                                                       const int* I, int node, int pn,
@@ -191,6 +196,8 @@ __device__ __forceinline__ void node_volume_direction(const StageArgs<N>& p, con
     const double j = __ldg(jrow[c]);
     hja_own[c] = HALF ? 0.5 * j : j;
   }
+  // lines of DIR inside one warp: N | 32 for DIR 0, N^2 | 32 for DIR 1
+  constexpr bool SHFL = WARP_ALL && (DIR == 0 ? 32 % N == 0 : DIR == 1 ? 32 % (N * N) == 0 : false);
   const double* Dm = &p.basis.Dsplit[m][0];
 #pragma unroll
   for (int o = 1; o < N; ++o) {
@@ -200,8 +207,15 @@ __device__ __forceinline__ void node_volume_direction(const StageArgs<N>& p, con
     double nrm[DIM];
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
-      const double jk = __ldg(jrow[c] + delta * SN);
-      nrm[c] = HALF ? hja_own[c] + 0.5 * jk : 0.5 * (hja_own[c] + jk);
+      if constexpr (SHFL) {
+        // the partner's own (halved when HALF) value: 0.5 * jk exactly
+        const double hjk =
+            __shfl_sync(0xffffffffu, hja_own[c], (int)(threadIdx.x & 31u) + delta * SN);
+        nrm[c] = HALF ? hja_own[c] + hjk : 0.5 * (hja_own[c] + hjk);
+      } else {
+        const double jk = __ldg(jrow[c] + delta * SN);
+        nrm[c] = HALF ? hja_own[c] + 0.5 * jk : 0.5 * (hja_own[c] + jk);
+      }
     }
     double f[NV];
     node_volume_flux<DIM, VF>(own, other, nrm, p.inv_gm1, hgm1, f);
@@ -464,17 +478,28 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   double acc[NV];
 #pragma unroll
   for (int q = 0; q < NV; ++q) acc[q] = 0.0;
-  if (active) {
-    const int* I = info + el * NI;
-    const double* U = us + el * NV * NDP;
-    const double* P = pr + el * NQ * NDP;
+  // blocks of whole warps run the volume term on every lane (lanes past the
+  // last element read element 0 and discard the result), so that the metric
+  // shuffles of node_volume_direction see full warps
+  constexpr bool WARP_ALL = NT % 32 == 0;
+  if (active || WARP_ALL) {
+    const int ev = active ? el : 0;
+    const int* I = info + ev * NI;
+    const double* U = us + ev * NV * NDP;
+    const double* P = pr + ev * NQ * NDP;
     const NodeFluxState<DIM> own = load_flux_state<DIM, VF>(U, P, NDP, pn);
     const double hgm1 = 0.5 * p.inv_gm1;
-    node_volume_direction<0, DIM, N, VF, NDP>(p, M, U, P, I, node, pn, own, hgm1, acc);
-    node_volume_direction<1, DIM, N, VF, NDP>(p, M, U, P, I, node, pn, own, hgm1, acc);
+    node_volume_direction<0, DIM, N, VF, NDP, WARP_ALL>(p, M, U, P, I, node, pn, own, hgm1, acc);
+    node_volume_direction<1, DIM, N, VF, NDP, WARP_ALL>(p, M, U, P, I, node, pn, own, hgm1, acc);
     if constexpr (DIM == 3)
-      node_volume_direction<2, DIM, N, VF, NDP>(p, M, U, P, I, node, pn, own, hgm1, acc);
-    if constexpr (HG) {
+      node_volume_direction<2, DIM, N, VF, NDP, WARP_ALL>(p, M, U, P, I, node, pn, own, hgm1,
+                                                          acc);
+  }
+  if constexpr (HG) {
+    if (active) {
+      const int* I = info + el * NI;
+      const double* U = us + el * NV * NDP;
+      const double* P = pr + el * NQ * NDP;
       // volume_flux.hpp:817-842: (1 - alpha) DG + alpha FV for troubled elements
       const double alpha = alpha_s[el];
       if (fabs(alpha - 0.0) > p.atol) {

@@ -207,16 +207,23 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
     double acc[NV];
 #pragma unroll
     for (int q = 0; q < NV; ++q) acc[q] = 0.0;
-    if (active) {
-      const int* I = info + el * NI;
-      const double* U = us + el * NV * NDP;
-      const double* P = pr + el * NQ * NDP;
+    // whole-warp volume term (see stage_node_body): lanes past the last
+    // element of a partial tile read element 0 and discard the result
+    constexpr bool WARP_ALL = NT % 32 == 0;
+    if (active || WARP_ALL) {
+      const int ev = active ? el : 0;
+      const int* I = info + ev * NI;
+      const double* U = us + ev * NV * NDP;
+      const double* P = pr + ev * NQ * NDP;
       const NodeFluxState<DIM> own = load_flux_state<DIM, VF>(U, P, NDP, pn);
       const double hgm1 = 0.5 * p.inv_gm1;
-      node_volume_direction<0, DIM, N, VF, NDP>(p, M, U, P, I, node, pn, own, hgm1, acc);
-      node_volume_direction<1, DIM, N, VF, NDP>(p, M, U, P, I, node, pn, own, hgm1, acc);
+      node_volume_direction<0, DIM, N, VF, NDP, WARP_ALL>(p, M, U, P, I, node, pn, own, hgm1,
+                                                          acc);
+      node_volume_direction<1, DIM, N, VF, NDP, WARP_ALL>(p, M, U, P, I, node, pn, own, hgm1,
+                                                          acc);
       if constexpr (DIM == 3)
-        node_volume_direction<2, DIM, N, VF, NDP>(p, M, U, P, I, node, pn, own, hgm1, acc);
+        node_volume_direction<2, DIM, N, VF, NDP, WARP_ALL>(p, M, U, P, I, node, pn, own,
+                                                            hgm1, acc);
     }
     __syncthreads();
 
