@@ -53,6 +53,12 @@ CASES = {
                       ic="vortex"),
     "ns": dict(ndims=2, polydeg=4, cells=(6, 6), left=(0.0, 0.0), right=(2 * math.pi,) * 2,
                ic="tgv2d", viscous=True, mu=1.0e-3, prandtl=0.72, noise=1.0e-3),
+    # element counts that leave the last block of the node-parallel shapes
+    # partly empty (8 and 2 elements per block): idle lanes in whole warps
+    "kh_hg_partial": dict(ndims=2, polydeg=3, cells=(5, 3), left=(-1.0, -1.0),
+                          right=(1.0, 1.0), ic="kh", shock_capturing=True, noise=0.05),
+    "tgv_partial": dict(ndims=3, polydeg=3, cells=(3, 3, 3), left=(0.0, 0.0, 0.0),
+                        right=(2 * math.pi,) * 3, ic="tgv3d"),
 }
 
 
