@@ -280,21 +280,19 @@ __device__ __forceinline__ void hllc_flux_2d(const FaceState<2>& Ls,
     const double sMuL = SL - vL, sMuR = SR - vR;
     const double SStar = (pR - pL + rL * vL * sMuL - rR * vR * sMuR) /
                          (rL * sMuL - rR * sMuR);
-    if (SStar >= 0.0) {
-      const double dS = rL * sMuL / (SL - SStar);
-      const double eS = EL / rL + (SStar - vL) * (SStar + pL / (rL * sMuL));
-      g[0] = mnL + SL * (dS - rL);
-      g[1] = (mnL * vL + pL) + SL * (dS * SStar - mnL);
-      g[2] = mnL * wL + SL * (dS * wL - mtL);
-      g[3] = vL * (EL + pL) + SL * (dS * eS - EL);
-    } else {
-      const double dS = rR * sMuR / (SR - SStar);
-      const double eS = ER / rR + (SStar - vR) * (SStar + pR / (rR * sMuR));
-      g[0] = mnR + SR * (dS - rR);
-      g[1] = (mnR * vR + pR) + SR * (dS * SStar - mnR);
-      g[2] = mnR * wR + SR * (dS * wR - mtR);
-      g[3] = vR * (ER + pR) + SR * (dS * eS - ER);
-    }
+    // star state of the side that SStar selects: the same expressions for
+    // both sides on selected operands, so the lanes of a warp that fall on
+    // different sides still run one branch
+    const bool l = SStar >= 0.0;
+    const double r = l ? rL : rR, sMu = l ? sMuL : sMuR, S = l ? SL : SR;
+    const double v = l ? vL : vR, w = l ? wL : wR, E = l ? EL : ER, p = l ? pL : pR;
+    const double mn = l ? mnL : mnR, mt = l ? mtL : mtR;
+    const double dS = r * sMu / (S - SStar);
+    const double eS = E / r + (SStar - v) * (SStar + p / (r * sMu));
+    g[0] = mn + S * (dS - r);
+    g[1] = (mn * v + p) + S * (dS * SStar - mn);
+    g[2] = mn * w + S * (dS * w - mt);
+    g[3] = v * (E + p) + S * (dS * eS - E);
   }
   f[0] = g[0] * nn;
   f[1] = (g[1] * nx - g[2] * ny) * nn;
