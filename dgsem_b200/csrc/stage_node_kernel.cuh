@@ -103,7 +103,9 @@ __device__ __forceinline__ NodeFluxState<DIM> load_flux_state(const double* U, c
 #pragma unroll
   for (int d = 0; d < DIM; ++d) s.v[d] = P[(K::V + d) * NDP + pn];
   s.p = P[K::P * NDP + pn];
-  s.hrho = K::HALF ? P[K::H_RHO * NDP + pn] : 0.0;
+  // Chandrashekar loads rho anyway: rho / 2 is exact, so derive it instead
+  // of a second shared-memory load (Kennedy-Gruber uses only rho / 2)
+  s.hrho = !K::HALF ? 0.0 : VF == VF_CHANDRASHEKAR ? 0.5 * s.rho : P[K::H_RHO * NDP + pn];
   s.x = K::HALF ? P[K::X * NDP + pn] : 0.0;
   s.y = VF == VF_CHANDRASHEKAR ? P[K::Y * NDP + pn] : 0.0;
   return s;
