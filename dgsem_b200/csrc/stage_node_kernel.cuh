@@ -107,7 +107,13 @@ __device__ __forceinline__ NodeFluxState<DIM> load_flux_state(const double* U, c
   // of a second shared-memory load (Kennedy-Gruber uses only rho / 2)
   s.hrho = !K::HALF ? 0.0 : VF == VF_CHANDRASHEKAR ? 0.5 * s.rho : P[K::H_RHO * NDP + pn];
   s.x = K::HALF ? P[K::X * NDP + pn] : 0.0;
-  s.y = VF == VF_CHANDRASHEKAR ? P[K::Y * NDP + pn] : 0.0;
+  // |v|^2 / 4 = sum (v_d / 2)^2 from the halved velocity, in the summation
+  // order of prepare_node: bit for bit the stored value, one load fewer
+  s.y = 0.0;
+  if constexpr (VF == VF_CHANDRASHEKAR) {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) s.y += s.v[d] * s.v[d];
+  }
   return s;
 }
 
