@@ -207,8 +207,15 @@ __device__ __forceinline__ void node_volume_direction(const StageArgs<N>& p, con
   // lines of DIR inside one warp: N | 32 for DIR 0, N^2 | 32 for DIR 1
   constexpr bool SHFL = WARP_ALL && (DIR == 0 ? 32 % N == 0 : DIR == 1 ? 32 % (N * N) == 0 : false);
   const double* Dm = &p.basis.Dsplit[m][0];
+  const int lane = (int)(threadIdx.x & 31u);
 #pragma unroll
   for (int o = 1; o < N; ++o) {
+    // With the line in one warp, the pair (m, m + o) for o < N - o is
+    // evaluated once, by node m, and handed on by shuffle to node m + o (the
+    // two-point flux and the pair normal are symmetric in the two nodes), so
+    // the partners o > N - o arrive from round N - o instead of being
+    // evaluated a second time.
+    if (SHFL && o > N - o) continue;
     const bool wrap = m + o >= N;
     const int delta = wrap ? o - N : o;  // k - m
     const NodeFluxState<DIM> other = load_flux_state<DIM, VF>(U, P, NDP, pn + delta * SP);
@@ -217,8 +224,7 @@ __device__ __forceinline__ void node_volume_direction(const StageArgs<N>& p, con
     for (int c = 0; c < DIM; ++c) {
       if constexpr (SHFL) {
         // the partner's own (halved when HALF) value: 0.5 * jk exactly
-        const double hjk =
-            __shfl_sync(0xffffffffu, hja_own[c], (int)(threadIdx.x & 31u) + delta * SN);
+        const double hjk = __shfl_sync(0xffffffffu, hja_own[c], lane + delta * SN);
         nrm[c] = HALF ? hja_own[c] + hjk : 0.5 * (hja_own[c] + hjk);
       } else {
         const double jk = __ldg(jrow[c] + delta * SN);
@@ -230,6 +236,14 @@ __device__ __forceinline__ void node_volume_direction(const StageArgs<N>& p, con
     const double dmk = Dm[m + delta];
 #pragma unroll
     for (int q = 0; q < NV; ++q) acc[q] += dmk * f[q];
+    if (SHFL && o < N - o) {
+      // f(m - o, m) from the node o back along the line (wrapping)
+      const int back = m - o < 0 ? N - o : -o;  // (m - o) mod N - m
+      const double dmb = Dm[m + back];
+#pragma unroll
+      for (int q = 0; q < NV; ++q)
+        acc[q] += dmb * __shfl_sync(0xffffffffu, f[q], lane + back * SN);
+    }
   }
 }
 
