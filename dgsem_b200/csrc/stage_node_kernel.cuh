@@ -71,13 +71,22 @@ struct NodeShape {
   static constexpr int SM_F = HG && 3 * EPB * ND > SM_F0 ? 3 * EPB * ND : SM_F0;
   static constexpr int SM_A = HG ? EPB : 0;        // alpha per element
   static constexpr int SM_VINV = HG ? N * N : 0;   // inverse Legendre Vandermonde
+  // volume-term exchange buffer [round][var][thread]: fluxes of the pairs
+  // (m, m+o), o = 1..XR, on x and y lines that do not lie in one warp (see
+  // node_volume_direction); lines inside a warp use shuffles instead, and z
+  // lines (3D) evaluate each pair twice (at n = 4 the exchange cost as much
+  // as it saved there and took shared memory from the persistent shape)
+  static constexpr int XR = (N - 1) / 2;
+  static constexpr bool WARP_ALL = (EPB * ND) % 32 == 0;
+  static constexpr bool XCHG = XR > 0 && (!WARP_ALL || 32 % N != 0 || 32 % (N * N) != 0);
+  static constexpr int SM_X = XCHG ? XR * NV * EPB * ND : 0;
   // staged u_n tile (one bulk copy) when a tile is a multiple of 16 bytes;
   // placed last so that launches without u_n (stage 1, RHS) can request
   // smem_bytes_base and leave the rest of the SM's storage to L1
   static constexpr int SM_N = (NV * ND) % 2 == 0 ? EPB * NV * ND : 0;
   static constexpr int NT = EPB * ND;
   static constexpr size_t smem_bytes_base =
-      sizeof(double) * (SM_U + SM_P + SM_F + SM_A + SM_VINV) + sizeof(int) * EPB * NI;
+      sizeof(double) * (SM_U + SM_P + SM_F + SM_A + SM_VINV + SM_X) + sizeof(int) * EPB * NI;
   static constexpr size_t off_n_bytes = (smem_bytes_base + 15) / 16 * 16;
   static constexpr size_t smem_bytes = off_n_bytes + sizeof(double) * SM_N;
 };
@@ -177,19 +186,23 @@ __device__ __forceinline__ void node_volume_flux(const NodeFluxState<DIM>& L,
   }
 }
 
-// Volume contribution of direction DIR to the node at padded position `pn`,
-// node index `node`, position m on its line.  WARP_ALL: every lane of the
-// calling warp executes the call (thread = element * n^d + node, blocks a
-// multiple of 32 threads); then, where a whole line of direction DIR lies in
-// one warp, the partners' metric terms come from the partners' lanes by
+// Volume contribution of direction DIR to the node at shared-memory position
+// `pn`, node index `node`, position m on its line.  WARP_ALL: every lane of
+// the calling warp executes the call (thread = element * n^d + node, blocks
+// a multiple of 32 threads); then, where a whole line of direction DIR lies
+// in one warp, the partners' metric terms come from the partners' lanes by
 // shuffle instead of a second global load (the same values, so the same
-// normal bit for bit).
-template <int DIR, int DIM, int N, int VF, int NDP, bool WARP_ALL = false>
+// normal bit for bit).  XB: the whole block executes the call and `xbuf`
+// holds (n-1)/2 * NV * nth doubles; pairs on lines that do not lie in one
+// warp are then shared through it (two block barriers per direction).
+template <int DIR, int DIM, int N, int VF, int NDP, bool WARP_ALL = false, bool XB = false>
 __device__ __forceinline__ void node_volume_direction(const StageArgs<N>& p, const MeshView& M,
                                                       const double* U, const double* P,
                                                       const int* I, int node, int pn,
                                                       const NodeFluxState<DIM>& own,
-                                                      double hgm1, double* acc) {
+                                                      double hgm1, double* acc,
+                                                      double* xbuf = nullptr, int tid = 0,
+                                                      int nth = 0) {
   constexpr int NV = DIM + 2, ND = ipow(N, DIM);
   constexpr bool HALF = NodeKernelSlots<DIM, VF>::HALF;
   // node-index and shared-memory-index strides along DIR
@@ -206,16 +219,18 @@ __device__ __forceinline__ void node_volume_direction(const StageArgs<N>& p, con
   }
   // lines of DIR inside one warp: N | 32 for DIR 0, N^2 | 32 for DIR 1
   constexpr bool SHFL = WARP_ALL && (DIR == 0 ? 32 % N == 0 : DIR == 1 ? 32 % (N * N) == 0 : false);
+  constexpr int XR = (N - 1) / 2;
+  constexpr bool XCHG = XB && !SHFL && XR > 0 && DIR < 2;
   const double* Dm = &p.basis.Dsplit[m][0];
   const int lane = (int)(threadIdx.x & 31u);
 #pragma unroll
   for (int o = 1; o < N; ++o) {
-    // With the line in one warp, the pair (m, m + o) for o < N - o is
-    // evaluated once, by node m, and handed on by shuffle to node m + o (the
-    // two-point flux and the pair normal are symmetric in the two nodes), so
-    // the partners o > N - o arrive from round N - o instead of being
+    // The pair (m, m + o) for o < N - o is evaluated once, by node m, and
+    // handed on to node m + o (by shuffle within a warp, else through xbuf):
+    // the two-point flux and the pair normal are symmetric in the two nodes,
+    // so the partners o > N - o arrive from round N - o instead of being
     // evaluated a second time.
-    if (SHFL && o > N - o) continue;
+    if ((SHFL || XCHG) && o > N - o) continue;
     const bool wrap = m + o >= N;
     const int delta = wrap ? o - N : o;  // k - m
     const NodeFluxState<DIM> other = load_flux_state<DIM, VF>(U, P, NDP, pn + delta * SP);
@@ -244,6 +259,22 @@ __device__ __forceinline__ void node_volume_direction(const StageArgs<N>& p, con
       for (int q = 0; q < NV; ++q)
         acc[q] += dmb * __shfl_sync(0xffffffffu, f[q], lane + back * SN);
     }
+    if (XCHG && o < N - o) {
+#pragma unroll
+      for (int q = 0; q < NV; ++q) xbuf[((o - 1) * NV + q) * nth + tid] = f[q];
+    }
+  }
+  if constexpr (XCHG) {
+    __syncthreads();
+#pragma unroll
+    for (int o = 1; o <= XR; ++o) {
+      const int back = m - o < 0 ? N - o : -o;
+      const double dmb = Dm[m + back];
+#pragma unroll
+      for (int q = 0; q < NV; ++q)
+        acc[q] += dmb * xbuf[((o - 1) * NV + q) * nth + tid + back * SN];
+    }
+    __syncthreads();  // the buffer is reused by the next direction
   }
 }
 
@@ -312,7 +343,8 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   double* sf = pr + S::SM_P;     // [el][face][fn][var]
   double* alpha_s = sf + S::SM_F;          // [el] (shock capturing)
   double* vinv_s = alpha_s + S::SM_A;      // [N][N] (shock capturing)
-  int* info = reinterpret_cast<int*>(vinv_s + S::SM_VINV);
+  double* xbuf = vinv_s + S::SM_VINV;      // volume-term exchange
+  int* info = reinterpret_cast<int*>(xbuf + S::SM_X);
   // [el][var][node] u_n tile (bulk-copy target; present when p.a != 0)
   double* stage_n = reinterpret_cast<double*>(reinterpret_cast<char*>(smem_node) + S::off_n_bytes);
 
@@ -504,18 +536,22 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   // last element read element 0 and discard the result), so that the metric
   // shuffles of node_volume_direction see full warps
   constexpr bool WARP_ALL = NT % 32 == 0;
-  if (active || WARP_ALL) {
+  static_assert(WARP_ALL == S::WARP_ALL, "thread count");
+  // with the exchange buffer every thread takes part (its barriers)
+  if (active || WARP_ALL || S::XCHG) {
     const int ev = active ? el : 0;
     const int* I = info + ev * NI;
     const double* U = us + ev * NV * NDP;
     const double* P = pr + ev * NQ * NDP;
     const NodeFluxState<DIM> own = load_flux_state<DIM, VF>(U, P, NDP, pn);
     const double hgm1 = 0.5 * p.inv_gm1;
-    node_volume_direction<0, DIM, N, VF, NDP, WARP_ALL>(p, M, U, P, I, node, pn, own, hgm1, acc);
-    node_volume_direction<1, DIM, N, VF, NDP, WARP_ALL>(p, M, U, P, I, node, pn, own, hgm1, acc);
+    node_volume_direction<0, DIM, N, VF, NDP, WARP_ALL, S::XCHG>(p, M, U, P, I, node, pn, own,
+                                                                hgm1, acc, xbuf, tid, NT);
+    node_volume_direction<1, DIM, N, VF, NDP, WARP_ALL, S::XCHG>(p, M, U, P, I, node, pn, own,
+                                                                hgm1, acc, xbuf, tid, NT);
     if constexpr (DIM == 3)
-      node_volume_direction<2, DIM, N, VF, NDP, WARP_ALL>(p, M, U, P, I, node, pn, own, hgm1,
-                                                          acc);
+      node_volume_direction<2, DIM, N, VF, NDP, WARP_ALL, S::XCHG>(p, M, U, P, I, node, pn, own,
+                                                                  hgm1, acc, xbuf, tid, NT);
   }
   if constexpr (HG) {
     if (active) {

@@ -8,7 +8,7 @@
 // contiguous range of the state).  Per tile:
 //   - u_in(t) has been requested by the previous iteration (or the prologue)
 //     as one bulk copy into `stage_in`, u_n(t) likewise into `stage_n`;
-//   - phase 1 converts stage_in into the padded tile + node data, after
+//   - phase 1 converts stage_in into the shared-memory tile + node data, after
 //     which one thread requests u_in(t + gridDim.x) into stage_in: the copy
 //     runs while faces, volume term and lifting of tile t are computed;
 //   - the epilogue waits for u_n(t), stores, and after the closing barrier
@@ -32,7 +32,8 @@ struct PipeShape {
                        NQ = B::NQ, NI = B::NI, NT = B::NT;
   static constexpr int SM_T = EPB * NV * ND;  // one staged tile (unpadded)
   static constexpr size_t smem_bytes =
-      sizeof(double) * (2 * SM_T + B::SM_U + B::SM_P + B::SM_F) + sizeof(int) * EPB * NI;
+      sizeof(double) * (2 * SM_T + B::SM_U + B::SM_P + B::SM_F + B::SM_X) +
+      sizeof(int) * EPB * NI;
   static constexpr bool kSupported = (NV * ND) % 2 == 0;
   // resident blocks per SM allowed by shared memory (228 KB, 1 KB reserved
   // per block), capped at 7 (72 registers per thread at 128 threads)
@@ -52,7 +53,8 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
   double* us = stage_n + S::SM_T;                  // [el][var][pnode]
   double* pr = us + S::B::SM_U;                    // [el][slot][pnode]
   double* sf = pr + S::B::SM_P;                    // [el][face][fn][var]
-  int* info = reinterpret_cast<int*>(sf + S::B::SM_F);
+  double* xbuf = sf + S::B::SM_F;                  // volume-term exchange
+  int* info = reinterpret_cast<int*>(xbuf + S::B::SM_X);
   __shared__ uint64_t bar_in, bar_n;
 
   stage_dependency_sync();
@@ -137,7 +139,7 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
       return;
     }
 
-    // ---- phase 1: tile -> padded tile + node data, sound speed, -1/J -------
+    // ---- phase 1: tile -> shared tile + node data, sound speed, -1/J -------
     if (active) {
       double u[NV];
 #pragma unroll
@@ -210,20 +212,21 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
     // whole-warp volume term (see stage_node_body): lanes past the last
     // element of a partial tile read element 0 and discard the result
     constexpr bool WARP_ALL = NT % 32 == 0;
-    if (active || WARP_ALL) {
+    constexpr bool XB = S::B::XCHG;  // exchange buffer: every thread takes part
+    if (active || WARP_ALL || XB) {
       const int ev = active ? el : 0;
       const int* I = info + ev * NI;
       const double* U = us + ev * NV * NDP;
       const double* P = pr + ev * NQ * NDP;
       const NodeFluxState<DIM> own = load_flux_state<DIM, VF>(U, P, NDP, pn);
       const double hgm1 = 0.5 * p.inv_gm1;
-      node_volume_direction<0, DIM, N, VF, NDP, WARP_ALL>(p, M, U, P, I, node, pn, own, hgm1,
-                                                          acc);
-      node_volume_direction<1, DIM, N, VF, NDP, WARP_ALL>(p, M, U, P, I, node, pn, own, hgm1,
-                                                          acc);
+      node_volume_direction<0, DIM, N, VF, NDP, WARP_ALL, XB>(p, M, U, P, I, node, pn, own, hgm1,
+                                                              acc, xbuf, tid, NT);
+      node_volume_direction<1, DIM, N, VF, NDP, WARP_ALL, XB>(p, M, U, P, I, node, pn, own, hgm1,
+                                                              acc, xbuf, tid, NT);
       if constexpr (DIM == 3)
-        node_volume_direction<2, DIM, N, VF, NDP, WARP_ALL>(p, M, U, P, I, node, pn, own,
-                                                            hgm1, acc);
+        node_volume_direction<2, DIM, N, VF, NDP, WARP_ALL, XB>(p, M, U, P, I, node, pn, own,
+                                                                hgm1, acc, xbuf, tid, NT);
     }
     __syncthreads();
 
@@ -265,7 +268,7 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
       if (bad) atomicOr(p.nonfinite, 1u);
     }
     __syncthreads();
-    // stage_n, padded tile, node data and face buffer are free again
+    // stage_n, shared tile, node data and face buffer are free again
     if (tid == 0 && with_n && t + (int)gridDim.x < ntiles)
       request(&bar_n, stage_n, M.u_n, t + gridDim.x);
   }
