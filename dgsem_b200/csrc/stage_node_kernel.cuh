@@ -12,9 +12,11 @@
 //      evaluate the flux in one argument order);
 //   2b one thread per node: for each direction, the two-point fluxes with the
 //      n-1 other nodes of its line, sum_k Dsplit(m, k) f(u_m, u_k, (Ja_m +
-//      Ja_k)/2), accumulated in registers (each pair is evaluated by both of
-//      its nodes: twice the flux work of the symmetric line loop, but no
-//      per-direction shared buffers and ~60 % of the registers);
+//      Ja_k)/2), accumulated in registers; the pair (m, m+o), o < n-o, is
+//      evaluated by node m and handed to node m+o by warp shuffle (lines
+//      inside one warp) or through a shared buffer (other x/y lines), z lines
+//      evaluate each pair at both nodes (~60 % of the registers of the line
+//      loop);
 //   3  lifting of the node's face fluxes, -1/J, SSPRK3 combination, store;
 //      the u_n tile of the combination is requested at kernel start as one
 //      bulk (TMA) copy into shared memory (16-byte-aligned states with an
