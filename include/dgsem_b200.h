@@ -268,13 +268,16 @@ dgsem_status dgsem_check_finite(dgsem_ctx* ctx);
 
 /* Launch-shape autotuner (no reference counterpart; the reference has one
  * fixed Kokkos launch shape).  The fused stage kernel has up to 6 launch
- * shapes: 0-2 line-parallel (elements per block, register cap; bitwise
- * identical results), 3-4 node-parallel with and without a register cap
- * (split form with or without shock capturing, not Navier-Stokes), 5
- * persistent node-parallel streaming element tiles through shared memory
- * with bulk copies (no shock capturing; 2D or even n in 3D; same results as
- * 3); 3-5 agree with 0-2 to rounding (same fluxes and the same alpha and
- * troubled-cell flags, different summation order).  dgsem_autotune times
+ * shapes: 0-2 line-parallel (elements per block, register cap), 3-4
+ * node-parallel with and without a register cap (split form with or without
+ * shock capturing, not Navier-Stokes), 5 persistent node-parallel streaming
+ * element tiles through shared memory with bulk copies (no shock capturing;
+ * 2D or even n in 3D).  The shapes of each group run the same source: their
+ * results agree bit for bit where the compiler emits the same arithmetic and
+ * to rounding where a register cap changes which multiply-adds it fuses
+ * (seen between 3 and 4 at n = 7 with the Ranocha flux); 3-5 agree with 0-2
+ * to rounding (same fluxes and the same alpha and troubled-cell flags,
+ * different summation order).  Every shape is deterministic.  dgsem_autotune times
  * one SSPRK3 step from state u (into the context temporaries; u is not
  * modified) with each available shape, 7 times in rounds that visit the
  * shapes in rotated order, keeps the one with the smallest median and returns
