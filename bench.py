@@ -108,32 +108,86 @@ KERNEL_DESCRIPTIONS = {
 }
 
 
-def profile_traffic(workload: str, kernel: str = "stage_kernel"):
-    """Per-launch DRAM bytes of the stage kernel from the committed ncu summary."""
+def profile_value(workload: str, kernel: str, key: str):
+    """A figure of the stage kernel's committed ncu summary (profiles/), e.g.
+    traffic_bytes_per_launch (DRAM read + write bytes of one launch) or
+    fp64_flops_per_dof (FP64 add + mul + 2 x fma thread operations per DOF
+    and stage)."""
     path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
     try:
         with open(path) as f:
             for line in f:
-                if line.startswith("traffic_bytes_per_launch:"):
+                if line.startswith(key + ":"):
                     return float(line.split(":", 1)[1].strip())
-    except OSError:
+    except (OSError, ValueError):
         pass
     return None
 
 
-class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+def profile_traffic(workload: str, kernel: str = "stage_kernel"):
+    return profile_value(workload, kernel, "traffic_bytes_per_launch")
 
+
+def fp64_peak(stream) -> dict:
+    """FP64 FMA throughput of this GPU measured live (dgsem_fp64_fma_peak:
+    CUDA-event-timed independent FMA chains on every SM, 2 FLOP per FMA)."""
+    import ctypes
+
+    from dgsem_b200 import _capi as C
+    fl, ms = ctypes.c_double(), ctypes.c_double()
+    C.check(C.lib().dgsem_fp64_fma_peak(ctypes.c_void_p(stream.cuda_stream), 4000,
+                                        ctypes.byref(fl), ctypes.byref(ms)), "fp64 peak")
+    return {"tflops": fl.value / 1e12, "ms": ms.value}
+
+
+class ClockSampler:
+    """SM clock, power and clock-event reasons sampled through NVML (read
+    only) every ~1 ms on a background thread while the timed region runs, so
+    that even a timed region of a few milliseconds gets samples; nvidia-smi
+    -lms 200 is the fallback when NVML cannot be loaded."""
+
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40,
+               "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device_index: int):
-        self.proc = None
+    def __init__(self, device_index: int, period_s: float = 0.001):
         self.dev = device_index
-        self.out = None
+        self.period = period_s
+        self.samples = []
+        self.smax = None
+        self._thread = None
+        self._stop = None
+        self._nvml = None
+        self.proc = None
+
+    def _poll(self, h):
+        import time as _t
+        nv = self._nvml
+        while not self._stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                mask = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((sm, mask))
+            except Exception:
+                pass
+            _t.sleep(self.period)
 
     def start(self):
+        import threading
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self.dev)
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self._nvml = nv
+            self._stop = threading.Event()
+            self._thread = threading.Thread(target=self._poll, args=(h,), daemon=True)
+            self._thread.start()
+            return
+        except Exception:
+            self._nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.QUERY}",
@@ -143,6 +197,16 @@ class ClockSampler:
             self.proc = None
 
     def stop(self):
+        if self._nvml is not None:
+            self._stop.set()
+            self._thread.join(timeout=5)
+            if not self.samples:
+                return None
+            reasons = {nm for nm, bit in self.REASONS.items()
+                       for _, mask in self.samples if mask & bit}
+            return {"sm_mhz": statistics.median(float(sm) for sm, _ in self.samples),
+                    "sm_max_mhz": self.smax, "reasons": sorted(reasons),
+                    "samples": len(self.samples), "source": "NVML, ~1 ms polling"}
         if self.proc is None:
             return None
         self.proc.terminate()
@@ -168,14 +232,32 @@ class ClockSampler:
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi -lms 200"}
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 # ---------------------------------------------------------------------------
 # reference arm / CPU baseline
 # ---------------------------------------------------------------------------
-def reference_rate(workload: str, budget_s: float, max_steps: int):
-    """Times the reference solver's CPU code (oracle/_ref) on the workload."""
+# One CPU sample policy for the reference arm and the device arm's
+# cpu_baseline leg: W untimed warm-up steps, then max(K, enough steps for
+# CPU_MIN_SAMPLE_S) timed steps, capped at CPU_MAX_SAMPLE_S of CPU time.
+CPU_MIN_SAMPLE_S = 5.0
+CPU_MAX_SAMPLE_S = 30.0
+
+
+def reference_case(workload: str):
+    """The reference solver (oracle/_ref) and the initial state of a workload."""
     from oracle import dgsem_oracle as do
     from oracle import ref_binding as rb
     nd, N, cells, left, right, vf, sf, ic, vi, bcs = WORKLOADS[workload]
@@ -187,52 +269,120 @@ def reference_rate(workload: str, budget_s: float, max_steps: int):
         kind = rb.EULER2D_PERIODIC_SPLIT
     rc = rb.RefCase(kind, N, cells, left, right, volume_flux=VF_CODE[vf],
                     surface_flux=SF_CODE[sf])
-    s_small = None
-    # initial state from the oracle's node coordinates formula at full size
-    s_small = do.Scheme(ndims=nd, polydeg=N, cells=cells, left=left, right=right,
-                        periodic=(bcs == "periodic"), bc=bcs if bcs == "dmr" else "periodic")
-    u = do.initial_state(s_small, ic)
+    s = do.Scheme(ndims=nd, polydeg=N, cells=cells, left=left, right=right,
+                  periodic=(bcs == "periodic"), bc=bcs if bcs == "dmr" else "periodic")
+    return rc, do.initial_state(s, ic)
+
+
+def reference_rate(workload: str, warmup: int, steps: int):
+    """Times the reference solver's CPU code (oracle/_ref) on the workload:
+    (DOF-updates/s, timed steps, seconds, threads, warm-up steps)."""
+    from oracle import ref_binding as rb
+    nd, N, cells = WORKLOADS[workload][:3]
+    rc, u = reference_case(workload)
     dt = time_step_size(workload)
-    u = rc.ssprk3(u, 0.0, dt, 1)  # warm-up step
     t0 = time.perf_counter()
-    u = rc.ssprk3(u, dt, dt, 1)
+    u = rc.ssprk3(u, 0.0, dt, 1)
     one = time.perf_counter() - t0
-    n = max(1, min(max_steps, int(budget_s / max(one, 1e-6))))
+    nwarm = max(1, min(warmup, int(0.5 * CPU_MAX_SAMPLE_S / max(one, 1e-6))))
+    if nwarm > 1:
+        u = rc.ssprk3(u, dt, dt, nwarm - 1)
     t0 = time.perf_counter()
-    rc.ssprk3(u, 2 * dt, dt, n)
+    u = rc.ssprk3(u, nwarm * dt, dt, 1)
+    one = time.perf_counter() - t0
+    n = max(steps, math.ceil(CPU_MIN_SAMPLE_S / max(one, 1e-6)))
+    n = max(1, min(n, int(CPU_MAX_SAMPLE_S / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    rc.ssprk3(u, (nwarm + 1) * dt, dt, n)
     el = time.perf_counter() - t0
     dofs = math.prod(cells) * (N + 1) ** nd
     threads = rb.lib().dgsem_ref_omp_threads()
-    return dofs * 3 * n / el, n, el, threads
+    return dofs * 3 * n / el, n, el, threads, nwarm
+
+
+def cpu_sample_text(workload: str, n: int, el: float, nwarm: int) -> str:
+    return (f"{nwarm} warm-up + {n} timed SSPRK3 steps of the full {workload} mesh "
+            f"({el:.1f} s; at least {CPU_MIN_SAMPLE_S:.0f} s, at most {CPU_MAX_SAMPLE_S:.0f} s "
+            f"of timed CPU work); reference src/ compiled with the project's Kokkos shim, "
+            f"OpenMP on all host threads; CPU: {cpu_model()}")
 
 
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    nd, N, cells = WORKLOADS[args.workload][:3]
     try:
-        rate, n, el, threads = reference_rate(args.workload, budget_s=60.0,
-                                              max_steps=max(args.steps, 1))
+        rate, n, el, threads, nwarm = reference_rate(args.workload, args.warmup, args.steps)
     except Exception as exc:  # reference library missing on this machine
         print(json.dumps({"impl": "reference", "unavailable": f"{type(exc).__name__}: {exc}"}))
         return 0
-    sample = (f"{n} SSPRK3 steps of the full {args.workload} mesh ({el:.1f} s, time-capped at "
-              f"60 s of the {args.steps} requested); reference src/ compiled with the project's "
-              f"Kokkos shim, OpenMP")
     line = {
         "metric": "FP64 DOF-updates/s per RHS", "value": rate, "unit": "DOF-updates/s",
-        "impl": "reference", "n_gpus": args.gpus, "steps": n, "warmup": 1,
+        "impl": "reference", "n_gpus": args.gpus, "steps": n, "warmup": args.warmup,
         "ms_per_step": 1e3 * el / n, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(args.workload),
         "cpu_baseline": {"value": rate, "unit": "DOF-updates/s", "cores": threads,
-                         "kind": "reference", "sample": sample},
+                         "kind": "reference", "cpu_model": cpu_model(),
+                         "sample": cpu_sample_text(args.workload, n, el, nwarm)},
         "e2e": {"value": rate, "unit": "DOF-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
     return 0
+
+
+def dmr_flag_check(solver, u, t, dt, dev, nsteps: int = 20):
+    """Troubled-cell flags of the GPU indicator against the reference's
+    HGIndicator (oracle/_ref, CPU) on the GPU's own stage inputs, over
+    `nsteps` further SSPRK3 steps of the double Mach reflection: per-stage
+    flagged counts, mismatches (must be 0) and the smallest distance of the
+    unclipped logistic alpha to the alpha_min decision (indicator.hpp:409-416;
+    flag = alpha > atol, volume_flux.hpp:772-773)."""
+    import ctypes
+
+    import torch
+
+    from dgsem_b200 import _capi as C
+    from oracle import dgsem_oracle as do
+    nd, N, cells, left, right = WORKLOADS["dmr"][:5]
+    rc, _ = reference_case("dmr")
+    s = do.Scheme(ndims=nd, polydeg=N, cells=cells, left=left, right=right, periodic=False,
+                  bc="dmr", shock_capturing=True, surface_flux="hllc")
+    atol = do.hg_atol()
+    L = C.lib()
+    ud = u.clone()
+    t1, t2 = torch.empty_like(ud), torch.empty_like(ud)
+
+    def p(x):
+        return ctypes.c_void_p(x.data_ptr()) if x is not None else None
+
+    def to_ref(x):
+        nx, ny = cells
+        return x.cpu().numpy().reshape(ny, nx, 4, -1).transpose(1, 0, 3, 2).copy()
+
+    flagged, mismatches, margin = [], 0, math.inf
+    for _ in range(nsteps):
+        for stage, (u_n, u_in, u_out) in enumerate(((None, ud, t1), (ud, t1, t2),
+                                                    (ud, t2, ud)), start=1):
+            _, flags = solver.indicator(u_in)
+            torch.cuda.synchronize()
+            uh = to_ref(u_in)
+            a_r = rc.alpha(uh).T.reshape(-1)
+            f_r = a_r > atol
+            f_d = flags.cpu().numpy().astype(bool)
+            mismatches += int((f_d != f_r).sum())
+            flagged.append(int(f_d.sum()))
+            raw = do.hg_alpha(s, uh, raw=True)
+            margin = min(margin, float(abs(raw - s.alpha_min).min()))
+            C.check(L.dgsem_ssprk3_stage(solver.handle, stage, p(u_n), p(u_in), p(u_out), t, dt),
+                    "stage")
+        t += dt
+    return {"stages_checked": len(flagged), "flagged_per_stage_min": min(flagged),
+            "flagged_per_stage_max": max(flagged), "flagged_per_stage": flagged,
+            "elements": math.prod(cells), "flag_mismatches": mismatches,
+            "min_abs_alpha_raw_minus_alpha_min": margin,
+            "checked_against": "reference HGIndicator (oracle/_ref) on the GPU stage inputs"}
 
 
 def max_over_ranks(local_ms: float, world: int, device) -> float:
@@ -386,6 +536,17 @@ def run_device_arm(args):
     peak, peak_kind = measured_peak()
     kernel = VARIANT_KERNELS.get(variant, "stage_kernel")
     traffic = profile_traffic(name, kernel)
+    # FP64 bound: FP64 operations per launch (ncu op counters of the committed
+    # summary, per DOF) over the same average launch time, against the FP64
+    # FMA peak measured live on this GPU
+    fpeak = fp64_peak(stream)
+    fpd = profile_value(name, kernel, "fp64_flops_per_dof")
+    fp64 = {"bound": "fp64", "peak": fpeak["tflops"], "unit": "TFLOP/s",
+            "peak_source": "measured live: dgsem_fp64_fma_peak (FMA chains, CUDA events)",
+            "flops_per_dof": fpd}
+    if fpd:
+        fp64["achieved"] = dofs * fpd / mean_stage_s / 1e12
+        fp64["frac"] = fp64["achieved"] / fpeak["tflops"]
 
     # e2e through the host-buffer C-ABI entry point (pinned host state)
     n_e2e = max(3, min(args.steps, 200))
@@ -423,32 +584,32 @@ def run_device_arm(args):
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (analytic initial condition of the workload)",
-        "config": dict(workload_config(name),
-                       parallelism=("replicas" if world > 1 else "single"),
-                       launch_variant=variant, variant_ms=variant_ms),
+        "config": workload_config(name),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs"
                      if peak_kind == "measured" else "fallback 6650 GB/s",
                      "kernel": KERNEL_DESCRIPTIONS[kernel],
-                     "algorithmic_bytes_per_launch": dofs * bpd},
+                     "algorithmic_bytes_per_launch": dofs * bpd, "fp64": fp64},
         "e2e": {"value": e2e_value, "unit": "DOF-updates/s", "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes, "steps": n_e2e,
                 "ms_per_step": statistics.mean(e2e_ms)},
         "gpu_launches": launches,
         "clocks": clocks,
-        "details": {"stage_ms_mean": [statistics.mean(x) for x in stage_ms],
+        "details": {"parallelism": "replicas" if world > 1 else "single",
+                    "launch_variant": variant, "variant_ms": variant_ms,
+                    "stage_ms_mean": [statistics.mean(x) for x in stage_ms],
                     "step_ms_median": statistics.median(step_ms),
                     "graph_step_ms_mean": graph_ms, "wall_s_timed_loop": wall},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            rate, n, el, threads = reference_rate(name, budget_s=args.cpu_budget,
-                                                  max_steps=10 ** 6)
+            rate, n, el, threads, nwarm = reference_rate(name, args.warmup, args.steps)
             line["cpu_baseline"] = {
                 "value": rate, "unit": "DOF-updates/s", "cores": threads, "kind": "reference",
-                "sample": f"{n} SSPRK3 steps of the full {name} mesh in {el:.1f} s; reference "
-                          f"src/ with the project's Kokkos shim, OpenMP"}
+                "cpu_model": cpu_model(), "sample": cpu_sample_text(name, n, el, nwarm)}
+            if name == "dmr":
+                line["details"]["troubled_cells"] = dmr_flag_check(solver, sol.u, t, dt, dev)
         except Exception as exc:
             line["cpu_baseline"] = {"value": None, "unavailable": f"{type(exc).__name__}: {exc}"}
     if rank == 0:
@@ -702,7 +863,6 @@ def main():
     ap.add_argument("--impl", default="dgsem_b200", choices=["dgsem_b200", "reference"])
     ap.add_argument("--workload", default="tgv16",
                     choices=list(WORKLOADS) + ["batched", "adjoint"])
-    ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variant", default="auto", choices=["auto", "0", "1", "2", "3", "4", "5"],
                     help="launch shape of the stage kernel (auto = autotuned)")

@@ -17,6 +17,8 @@ STATUS_NAMES = {0: "ok", 1: "invalid argument", 2: "unsupported combination",
                 3: "CUDA error", 4: "non-finite value in state",
                 5: "device wait timed out", 6: "allocation failed",
                 7: "state larger than the static scratch"}
+DGSEM_ERR_INVALID_ARG, DGSEM_ERR_UNSUPPORTED, DGSEM_ERR_CUDA = 1, 2, 3
+DGSEM_ERR_NONFINITE, DGSEM_ERR_TIMEOUT, DGSEM_ERR_ALLOC = 4, 5, 6
 DGSEM_ERR_SCRATCH_LIMIT = 7
 STATIC_SCRATCH_MAX_STATE = 2097152  # DGSEM_STATIC_SCRATCH_MAX_STATE (doubles per stage state)
 
@@ -45,6 +47,7 @@ EXPORTED = [
     "dgsem_batch_autotune", "dgsem_ssprk3_step_static_scratch",
     "dgsem_adjoint_create", "dgsem_adjoint_destroy", "dgsem_adjoint_rhs_vjp",
     "dgsem_kinetic_energy", "dgsem_adjoint_gradient", "dgsem_coordinates_host",
+    "dgsem_fp64_fma_peak",
 ]
 
 
@@ -131,6 +134,7 @@ def lib() -> ctypes.CDLL:
     L.dgsem_kinetic_energy.argtypes = [vp, dp, c.POINTER(c.c_double), dp]
     L.dgsem_adjoint_gradient.argtypes = [vp, dp, c.c_double, c.c_double,
                                          c.POINTER(c.c_double), dp]
+    L.dgsem_fp64_fma_peak.argtypes = [vp, c.c_int, c.POINTER(c.c_double), c.POINTER(c.c_double)]
     for name in EXPORTED:
         f = getattr(L, name)
         if name != "dgsem_status_string":

@@ -198,11 +198,26 @@ dgsem_status validate(const dgsem_mesh_desc* m, const dgsem_scheme_desc* s) {
   return DGSEM_OK;
 }
 
+// Failure-path testing: with DGSEM_TEST_FAIL_ALLOC_AT=k in the environment
+// at context creation, the k-th device allocation of that creation (1-based)
+// fails as if cudaMalloc had run out of memory.
+int test_fail_alloc_at() {
+  const char* v = std::getenv("DGSEM_TEST_FAIL_ALLOC_AT");
+  return v ? std::atoi(v) : 0;
+}
+
 template <class T>
 T* device_alloc(dgsem_ctx* ctx, size_t count, cudaError_t* err) {
   void* p = nullptr;
+  if (++ctx->alloc_calls == ctx->fail_alloc_at) {
+    *err = cudaErrorMemoryAllocation;
+    return nullptr;
+  }
   *err = cudaMalloc(&p, count * sizeof(T));
-  if (*err != cudaSuccess) return nullptr;
+  if (*err != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
   ctx->allocations.push_back(p);
   return static_cast<T*>(p);
 }
@@ -254,6 +269,7 @@ dgsem_status dgsem_ctx_create(const dgsem_mesh_desc* mesh,
   ctx->mesh = *mesh;
   ctx->scheme = *scheme;
   ctx->stream = static_cast<cudaStream_t>(stream);
+  ctx->fail_alloc_at = test_fail_alloc_at();
   cudaGetDevice(&ctx->device);
   ctx->engine = std::move(engine);
   EngineConfig& c = ctx->cfg;
@@ -265,6 +281,14 @@ dgsem_status dgsem_ctx_create(const dgsem_mesh_desc* mesh,
     c.periodic[a] = a < nd ? (scheme->bc[2 * a] == DGSEM_BC_PERIODIC) : 1;
     c.nelem *= c.cells[a];
   }
+  // Failure-path testing only: DGSEM_TEST_WAIT_LIMIT_NS bounds the stage
+  // kernels' tile-copy waits (default 1 s); DGSEM_TEST_SKIP_TILE_COPY=1 makes
+  // the node-parallel kernels arm the u_n barrier without issuing the copy,
+  // so the bounded wait runs out (DGSEM_ERR_TIMEOUT from dgsem_check_finite)
+  // with no copy in flight.
+  if (const char* v = std::getenv("DGSEM_TEST_WAIT_LIMIT_NS"))
+    c.wait_limit_ns = std::strtoull(v, nullptr, 10);
+  if (const char* v = std::getenv("DGSEM_TEST_SKIP_TILE_COPY")) c.skip_tile_copy = std::atoi(v);
   c.gamma = scheme->gamma;
   c.mu = scheme->mu;
   c.prandtl = scheme->prandtl > 0 ? scheme->prandtl : 0.72;

@@ -29,4 +29,7 @@ struct dgsem_ctx {
   double* table_block = nullptr;
   unsigned int* flag = nullptr;
   int64_t launches = 0;
+  // failure-path testing: allocation number that fails (0 = none)
+  int alloc_calls = 0;
+  int fail_alloc_at = 0;
 };

@@ -36,6 +36,9 @@ struct EngineConfig {
   BasisTables basis;
   unsigned int* nonfinite;  // device flag
   double* grad;             // Navier-Stokes lifted gradient [E][4][2][n^2]
+  // failure-path testing (StageArgs::wait_limit_ns / skip_tile_copy)
+  unsigned long long wait_limit_ns;
+  int skip_tile_copy;
 };
 
 // Launch-shape variants: 0-2 line-parallel (stage_kernel.cuh), 3-4
@@ -279,6 +282,8 @@ class Engine final : public EngineBase {
     args.mu = cfg.mu;
     args.kappa = cfg.gamma / ((cfg.gamma - 1.0) * cfg.prandtl);
     args.bc = cfg.bc;
+    args.wait_limit_ns = cfg.wait_limit_ns;
+    args.skip_tile_copy = cfg.skip_tile_copy;
     fill_basis_const<N>(cfg.basis, &args.basis);
     return args;
   }

@@ -99,6 +99,12 @@ struct StageArgs {
   double mu, kappa;
   BcParams bc;
   BasisConst<N> basis;
+  // Failure-path testing only (both 0 in normal use): bound of the tile-copy
+  // waits in ns (0 = 1 s) and, when skip_tile_copy is set, the node-parallel
+  // kernel arms its u_n barrier without issuing the copy, so that the wait
+  // runs out with nothing in flight.
+  unsigned long long wait_limit_ns;
+  int skip_tile_copy;
 };
 
 // ---------------------------------------------------------------------------

@@ -380,7 +380,7 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
     mbar_init(&bar_n, 1);
     mbar_fence_init();
     mbar_arrive_expect_tx(&bar_n, bytes);
-    bulk_copy_g2s(stage_n, M.u_n + (int64_t)e0 * NV * ND, bytes, &bar_n);
+    if (!p.skip_tile_copy) bulk_copy_g2s(stage_n, M.u_n + (int64_t)e0 * NV * ND, bytes, &bar_n);
   }
 
   // ---- phase 0: element info and the u_in tile --------------------------
@@ -573,7 +573,7 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   }
   __syncthreads();
   // the block agrees on a timeout (vote) so that all of it leaves together
-  if (bulk_n && __syncthreads_or(!mbar_wait_bounded(&bar_n, 0))) {
+  if (bulk_n && __syncthreads_or(!mbar_wait_bounded(&bar_n, 0, p.wait_limit_ns))) {
     if (tid == 0) atomicOr(p.nonfinite, 2u);
     return;
   }

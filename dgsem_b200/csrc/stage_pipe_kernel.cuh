@@ -134,7 +134,7 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
       }
     }
     // the block agrees on a timeout (vote) so that all of it leaves together
-    if (__syncthreads_or(!mbar_wait_bounded(&bar_in, phase))) {
+    if (__syncthreads_or(!mbar_wait_bounded(&bar_in, phase, p.wait_limit_ns))) {
       if (tid == 0) atomicOr(p.nonfinite, 2u);
       return;
     }
@@ -231,7 +231,7 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
     __syncthreads();
 
     // ---- phase 3: lifting, -1/J, SSPRK3 combination, store -----------------
-    if (with_n && __syncthreads_or(!mbar_wait_bounded(&bar_n, phase))) {
+    if (with_n && __syncthreads_or(!mbar_wait_bounded(&bar_n, phase, p.wait_limit_ns))) {
       if (tid == 0) atomicOr(p.nonfinite, 2u);
       return;
     }

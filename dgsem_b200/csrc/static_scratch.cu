@@ -12,6 +12,7 @@
 
 #include <mutex>
 
+#include "context.hpp"
 #include "dgsem_b200.h"
 
 // Two stage states of at most DGSEM_STATIC_SCRATCH_MAX_STATE doubles each
@@ -24,25 +25,24 @@ namespace {
 
 constexpr int kMaxDevices = 64;
 
-// Per-device address of the scratch, looked up once with that device current.
-struct ScratchSlot {
-  std::once_flag once;
-  double* ptr = nullptr;
-  cudaError_t err = cudaSuccess;
-};
-
-ScratchSlot g_slots[kMaxDevices];
+// Per-device address of the scratch, looked up with that device current.
+// Only a successful look-up is kept: a failed one (which leaves nothing
+// cached) is retried by the next call on that device.
+std::mutex g_slot_mutex;
+double* g_slots[kMaxDevices] = {};
 
 dgsem_status scratch_on_device(int device, double** out) {
   if (device < 0 || device >= kMaxDevices) return DGSEM_ERR_INVALID_ARG;
-  ScratchSlot& s = g_slots[device];
-  std::call_once(s.once, [&s]() {
+  std::lock_guard<std::mutex> lock(g_slot_mutex);
+  if (!g_slots[device]) {
     void* p = nullptr;
-    s.err = cudaGetSymbolAddress(&p, dgsem_stage_scratch);
-    s.ptr = s.err == cudaSuccess ? static_cast<double*>(p) : nullptr;
-  });
-  if (s.err != cudaSuccess || !s.ptr) return DGSEM_ERR_CUDA;
-  *out = s.ptr;
+    if (cudaGetSymbolAddress(&p, dgsem_stage_scratch) != cudaSuccess || !p) {
+      cudaGetLastError();  // leave no stale error for the next launch check
+      return DGSEM_ERR_CUDA;
+    }
+    g_slots[device] = static_cast<double*>(p);
+  }
+  *out = g_slots[device];
   return DGSEM_OK;
 }
 
@@ -56,11 +56,19 @@ extern "C" dgsem_status dgsem_ssprk3_step_static_scratch(dgsem_ctx* ctx, double*
   dgsem_status st = dgsem_get_sizes(ctx, &nelem, &nodes, &nvars, &state_len);
   if (st != DGSEM_OK) return st;
   if (state_len > DGSEM_STATIC_SCRATCH_MAX_STATE) return DGSEM_ERR_SCRATCH_LIMIT;
-  // The scratch address is per device: u must live on the current device.
+  // The scratch address is per device: u and the context must belong to
+  // the current device.
   int device = -1;
-  if (cudaGetDevice(&device) != cudaSuccess) return DGSEM_ERR_CUDA;
+  if (cudaGetDevice(&device) != cudaSuccess) {
+    cudaGetLastError();
+    return DGSEM_ERR_CUDA;
+  }
+  if (ctx->device != device) return DGSEM_ERR_INVALID_ARG;
   cudaPointerAttributes attr;
-  if (cudaPointerGetAttributes(&attr, u) != cudaSuccess) return DGSEM_ERR_CUDA;
+  if (cudaPointerGetAttributes(&attr, u) != cudaSuccess) {
+    cudaGetLastError();
+    return DGSEM_ERR_INVALID_ARG;
+  }
   if ((attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged) ||
       attr.device != device)
     return DGSEM_ERR_INVALID_ARG;

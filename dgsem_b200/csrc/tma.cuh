@@ -66,14 +66,20 @@ __device__ __forceinline__ uint64_t global_timer_ns() {
   return t;
 }
 
-// Waits for phase `parity` of `bar` for at most ~1 s of wall time (and at
-// most 2^30 polls); returns false on timeout (the caller reports it).
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+// Default bound of an mbarrier wait: 1 s of wall time.
+constexpr uint64_t kWaitLimitNs = 1000000000ull;
+
+// Waits for phase `parity` of `bar` for at most `limit_ns` of wall time
+// (kWaitLimitNs when 0) and at most 2^30 polls; returns false on timeout
+// (the caller reports it).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
+                                                  uint64_t limit_ns = 0) {
   if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t limit = limit_ns ? limit_ns : kWaitLimitNs;
   const uint64_t t0 = global_timer_ns();
   for (uint32_t i = 0; i < (1u << 30); ++i) {
     if (mbar_try_wait(bar, parity)) return true;
-    if (global_timer_ns() - t0 > 1000000000ull) return false;
+    if (global_timer_ns() - t0 > limit) return false;
   }
   return false;
 }

@@ -173,11 +173,14 @@ dgsem_status dgsem_ssprk3_steps(dgsem_ctx* ctx, double* u, double t0,
  *  - Limit: the state may hold at most DGSEM_STATIC_SCRATCH_MAX_STATE doubles
  *    (2^21, 16 MiB; the scratch is 2 x 16 MiB per device); larger states
  *    return DGSEM_ERR_SCRATCH_LIMIT and launch nothing.
- *  - u must be device memory of the CURRENT device (else
- *    DGSEM_ERR_INVALID_ARG), and the context must belong to that device.
+ *  - u must be device memory of the CURRENT device and the context must
+ *    have been created with that device current; otherwise (a host pointer,
+ *    another device's memory or context) DGSEM_ERR_INVALID_ARG.
  *  - The first call on a device is its set-up: it looks up the scratch's
  *    address (cudaGetSymbolAddress, which may load the module that holds
- *    the scratch).  Make that first call before any stream capture.
+ *    the scratch).  Make that first call before any stream capture.  A
+ *    failed set-up returns DGSEM_ERR_CUDA, clears the CUDA error state and
+ *    is tried again by the next call.
  *  - Nothing has to start at zero: each stage state is fully written before
  *    it is read.
  *  - There is ONE scratch per device, shared by every context: two calls
@@ -334,6 +337,15 @@ dgsem_status dgsem_kinetic_energy(dgsem_adjoint* adj, const double* u,
 dgsem_status dgsem_adjoint_gradient(dgsem_adjoint* adj, const double* u0,
                                     double t0, double dt, double* value,
                                     double* grad_u0);
+
+/* FP64 fused-multiply-add throughput of the current device (no reference
+ * counterpart: the reference has no timers): one warm-up and one timed
+ * launch of `iters` x 128 independent FMAs per thread on every SM, timed
+ * with CUDA events on `stream` (a cudaStream_t).  *flops_per_s receives
+ * 2 x FMAs / s (the FP64-pipe bound of the roofline), *ms the launch time
+ * (may be NULL).  Synchronous; changes no clock or power setting. */
+dgsem_status dgsem_fp64_fma_peak(void* stream, int iters, double* flops_per_s,
+                                 double* ms);
 
 /* Host-side copies of the basis tables (nodes, weights, inv_weights,
  * lhat(-1), lhat(+1), D, Dsplit, Dhat, inverse Legendre Vandermonde; the

@@ -701,10 +701,13 @@ def _grid(s: Scheme, a):
     return a.reshape(cells + (s.n,) * nd + a.shape[nd + 1:])
 
 
-def hg_alpha(s: Scheme, u):
+def hg_alpha(s: Scheme, u, raw: bool = False):
     """subcell_limiting/indicator.hpp:313-428 (2D) / :430-585 (3D).
 
-    Indicator rho*p with gamma fixed to 1.4 (indicator.hpp:137-210).
+    Indicator rho*p with gamma fixed to 1.4 (indicator.hpp:137-210).  With
+    raw=True the logistic alpha before the alpha_min / alpha_max clipping
+    (indicator.hpp:409-416) is returned: the troubled-cell decision is
+    raw >= alpha_min, so |raw - alpha_min| is its margin.
     """
     n = s.n
     nd = s.ndims
@@ -795,6 +798,8 @@ def hg_alpha(s: Scheme, u):
     arg = -sfac / threshold * (energy - threshold)
     ex = np.vectorize(math.exp, otypes=[np.float64])(arg)
     alpha = 1.0 / (1.0 + ex)
+    if raw:
+        return alpha
     alpha = np.where(alpha < s.alpha_min, 0.0, alpha)
     alpha = np.where(alpha > 1.0 - s.alpha_min, 1.0, alpha)
     return np.minimum(s.alpha_max, alpha)

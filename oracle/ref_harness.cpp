@@ -361,6 +361,33 @@ class RefCase final : public RefCaseBase {
   std::unique_ptr<DGSEM::SSPRK3<T, Solver, Mesh, Sol>> integrator_;
 };
 
+// 2D shock capturing (VolumeIntegralShockCapturingHG with the reference's
+// LaxFriedrichsFlux for the FV subcells) with the volume flux chosen by
+// c.volume_flux and the surface flux by c.surface_flux.  The plugin volume
+// fluxes are instantiated at polydeg 3 (the benchmark degree) only, to bound
+// the build time.
+template <std::size_t N, template <class> class VFlux, class Bcs>
+RefCaseBase* make_hg_2d_vf(const dgsem_ref_case& c, const DGSEM::equations::CompressibleEuler2D<T>& eq,
+                           const Bcs& b, bool periodic) {
+  using Basis = DGSEM::Basis::LobattoLegendreBasis<T, N>;
+  using E2 = DGSEM::equations::CompressibleEuler2D<T>;
+  using VF = DGSEM::VolumeIntegralShockCapturingHG<Basis, E2, VFlux, DGSEM::LaxFriedrichsFlux,
+                                                   DGSEM::HGIndicator<Basis, E2>>;
+  if (c.surface_flux == 1) return new RefCase<E2, N, VF, Bcs, 2, HLLC2DPlugin>(c, eq, b, periodic);
+  return new RefCase<E2, N, VF, Bcs, 2>(c, eq, b, periodic);
+}
+
+template <std::size_t N, class Bcs>
+RefCaseBase* make_hg_2d(const dgsem_ref_case& c, const DGSEM::equations::CompressibleEuler2D<T>& eq,
+                        const Bcs& b, bool periodic) {
+  if constexpr (N == 3) {
+    if (c.volume_flux == 1) return make_hg_2d_vf<N, RanochaPlugin>(c, eq, b, periodic);
+    if (c.volume_flux == 2) return make_hg_2d_vf<N, KennedyGruberPlugin>(c, eq, b, periodic);
+  }
+  if (c.volume_flux != 0) return nullptr;
+  return make_hg_2d_vf<N, DGSEM::ChandrashekarFlux>(c, eq, b, periodic);
+}
+
 template <std::size_t N>
 RefCaseBase* make_case_n(const dgsem_ref_case& c) {
   using Basis = DGSEM::Basis::LobattoLegendreBasis<T, N>;
@@ -384,26 +411,16 @@ RefCaseBase* make_case_n(const dgsem_ref_case& c) {
       return new RefCase<E2, N, VF, decltype(b), 2>(c, E2{c.gamma}, b, true);
     }
     case REF_EULER2D_PERIODIC_HG: {
-      using VF = DGSEM::VolumeIntegralShockCapturingHG<
-          Basis, E2, DGSEM::ChandrashekarFlux, DGSEM::LaxFriedrichsFlux,
-          DGSEM::HGIndicator<Basis, E2>>;
       auto b = DGSEM::BoundarySet(P{}, P{}, P{}, P{});
-      if (c.surface_flux == 1)
-        return new RefCase<E2, N, VF, decltype(b), 2, HLLC2DPlugin>(c, E2{c.gamma}, b, true);
-      return new RefCase<E2, N, VF, decltype(b), 2>(c, E2{c.gamma}, b, true);
+      return make_hg_2d<N>(c, E2{c.gamma}, b, true);
     }
     case REF_EULER2D_DMR_HG: {
-      using VF = DGSEM::VolumeIntegralShockCapturingHG<
-          Basis, E2, DGSEM::ChandrashekarFlux, DGSEM::LaxFriedrichsFlux,
-          DGSEM::HGIndicator<Basis, E2>>;
       DmrBoundaryState inflow{c.gamma};
       auto b = DGSEM::BoundarySet(
           DGSEM::DirichletBC(inflow), DGSEM::OutflowBC{},
           DGSEM::MixedDirichletSlipWallBC(inflow, DmrBottomInflow{}),
           DGSEM::DirichletBC(inflow));
-      if (c.surface_flux == 1)
-        return new RefCase<E2, N, VF, decltype(b), 2, HLLC2DPlugin>(c, E2{c.gamma}, b, false);
-      return new RefCase<E2, N, VF, decltype(b), 2>(c, E2{c.gamma}, b, false);
+      return make_hg_2d<N>(c, E2{c.gamma}, b, false);
     }
     case REF_EULER3D_PERIODIC_SPLIT: {
       auto b = DGSEM::BoundarySet(P{}, P{}, P{}, P{}, P{}, P{});

@@ -1,0 +1,230 @@
+"""Parity at the benchmark sizes against the reference's own assembly.
+
+The compiled reference (oracle/_ref: the reference's src/ with the project's
+Kokkos shim) runs its StructuredSolver::calc_rhs, HGIndicator and boundary
+assembly; the fluxes it does not ship (Ranocha, Kennedy-Gruber, 2D HLLC)
+enter it as plugin structs with its numerical_flux(eq, uL, uR, normal)
+signature (oracle/ref_harness.cpp), so assembly, lifting, metrics and
+boundaries are the reference's code in every case below.
+
+* TGV 16^3, N = 3, Kennedy-Gruber + LLF (the headline workload), every
+  launch shape, at the initial state and after 50 GPU steps;
+* KH 64^2, N = 3, Ranocha + LLF, at the initial state and after 100 steps;
+* DMR 240 x 60, N = 3, HG shock capturing + HLLC, every stage of 200 GPU
+  steps: identical troubled-cell flags and alpha, and the RHS of the final
+  state; the per-stage flagged counts and the smallest distance of the
+  logistic alpha to the alpha_min decision are printed;
+* the small shock-capturing and 3D cases of the other-flux tests against the
+  reference assembly with the same plugins.
+
+Bar: RHS relative L-infinity <= RTOL (1e-12); flags identical.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+import pytest
+
+from oracle import dgsem_oracle as do
+from oracle import ref_binding as rb
+from tests._util import CASES, RTOL, alpha_ref_to_dev, dev_to_ref, ref_to_dev, rel_linf
+
+pytestmark = pytest.mark.gpu
+
+VFC = {"chandrashekar": 0, "ranocha": 1, "kennedy_gruber": 2}
+SFC = {"llf": 0, "hllc": 1}
+
+
+def _need_ref():
+    if not rb.available():
+        pytest.skip("compiled reference not built")
+
+
+def _solver(nd, N, cells, left, right, vf, sf, hg=False, dmr=False):
+    import dgsem_b200 as D
+    mesh = D.StructuredMesh(left, right, cells)
+    eq = D.CompressibleEuler3D(1.4) if nd == 3 else D.CompressibleEuler2D(1.4)
+    flux = {"chandrashekar": D.ChandrashekarFlux, "ranocha": D.RanochaFlux,
+            "kennedy_gruber": D.KennedyGruberFlux}[vf]
+    vi = D.VolumeIntegralShockCapturingHG(flux) if hg else D.VolumeIntegralSplitForm(flux)
+    sflux = D.HLLCFlux() if sf == "hllc" else D.LaxFriedrichsFlux()
+    if dmr:
+        bcs = D.BoundarySet(D.DirichletBC("double_mach"), D.OutflowBC(),
+                            D.MixedDirichletSlipWallBC("double_mach"),
+                            D.DirichletBC("double_mach"))
+    else:
+        bcs = D.BoundarySet(*[D.PeriodicBC() for _ in range(2 * nd)])
+    solver = D.StructuredSolver(eq, D.LobattoLegendreBasis(N), vi, sflux, mesh, bcs)
+    if hg:
+        solver.set_indicator_parameters(0.5, 0.001, False)
+    return solver
+
+
+def _rhs(solver, u_dev, t):
+    import torch
+    du = torch.empty_like(u_dev)
+    solver.rhs(u_dev, du, t)
+    torch.cuda.synchronize()
+    return dev_to_ref(du.cpu().numpy(), solver.mesh.n_cells)
+
+
+def _steps(solver, u_dev, t0, dt, n):
+    from dgsem_b200 import _capi as C
+    C.check(C.lib().dgsem_ssprk3_steps(solver.handle, ctypes.c_void_p(u_dev.data_ptr()), t0, dt,
+                                       n), "dgsem_ssprk3_steps")
+
+
+def test_tgv16_kennedy_gruber_every_shape_matches_reference(cuda):
+    import torch
+    _need_ref()
+    cells, left, right = (16, 16, 16), (0.0,) * 3, (2 * math.pi,) * 3
+    s = do.Scheme(ndims=3, polydeg=3, cells=cells, left=left, right=right,
+                  volume_flux="kennedy_gruber")
+    u0 = do.initial_state(s, "tgv3d")
+    rc = rb.RefCase(rb.EULER3D_PERIODIC_SPLIT, 3, cells, left, right, volume_flux=2)
+    solver = _solver(3, 3, cells, left, right, "kennedy_gruber", "llf")
+    ud = torch.from_numpy(ref_to_dev(u0, 3)).to(cuda)
+    du_r = rc.rhs(u0, 0.0)
+    nshapes = 6
+    for v in range(nshapes):
+        solver.set_launch_variant(v)
+        err = rel_linf(_rhs(solver, ud, 0.0), du_r)
+        assert err <= RTOL, (v, err)
+    # after 50 steps of the reference TGV time step (the workload's run)
+    dt = 0.1 * (2 * math.pi / 16) / 2.0 / (3.0 * 7)
+    solver.autotune(ud)
+    _steps(solver, ud, 0.0, dt, 50)
+    torch.cuda.synchronize()
+    u50 = dev_to_ref(ud.cpu().numpy(), cells)
+    du_r = rc.rhs(u50, 50 * dt)
+    for v in range(nshapes):
+        solver.set_launch_variant(v)
+        err = rel_linf(_rhs(solver, ud, 50 * dt), du_r)
+        assert err <= RTOL, (v, err)
+
+
+def test_kh64_ranocha_matches_reference(cuda):
+    import torch
+    _need_ref()
+    cells, left, right = (64, 64), (-1.0, -1.0), (1.0, 1.0)
+    s = do.Scheme(ndims=2, polydeg=3, cells=cells, left=left, right=right,
+                  volume_flux="ranocha")
+    u0 = do.initial_state(s, "kh")
+    rc = rb.RefCase(rb.EULER2D_PERIODIC_SPLIT, 3, cells, left, right, volume_flux=1)
+    solver = _solver(2, 3, cells, left, right, "ranocha", "llf")
+    ud = torch.from_numpy(ref_to_dev(u0, 2)).to(cuda)
+    du_r = rc.rhs(u0, 0.0)
+    for v in range(6):
+        solver.set_launch_variant(v)
+        assert rel_linf(_rhs(solver, ud, 0.0), du_r) <= RTOL, v
+    dt = 0.5 * (2.0 / 64) / (7.0 * 1.84)  # CFL 0.5, the workload's time step
+    solver.autotune(ud)
+    _steps(solver, ud, 0.0, dt, 100)
+    torch.cuda.synchronize()
+    u100 = dev_to_ref(ud.cpu().numpy(), cells)
+    du_r = rc.rhs(u100, 100 * dt)
+    for v in range(6):
+        solver.set_launch_variant(v)
+        assert rel_linf(_rhs(solver, ud, 100 * dt), du_r) <= RTOL, v
+
+
+def test_dmr_developed_shock_flags_and_rhs_match_reference(cuda):
+    """Every stage of 200 steps (the workload's run, CFL 0.4 with lambda_max
+    = 12): the GPU indicator's flags equal the reference HGIndicator's on the
+    GPU's own stage input; then the RHS of the developed state."""
+    import torch
+
+    from dgsem_b200 import _capi as C
+    _need_ref()
+    cells, left, right = (240, 60), (0.0, 0.0), (4.0, 1.0)
+    s = do.Scheme(ndims=2, polydeg=3, cells=cells, left=left, right=right, periodic=False,
+                  bc="dmr", shock_capturing=True, surface_flux="hllc")
+    u0 = do.initial_state(s, "dmr")
+    rc = rb.RefCase(rb.EULER2D_DMR_HG, 3, cells, left, right, surface_flux=1)
+    solver = _solver(2, 3, cells, left, right, "chandrashekar", "hllc", hg=True, dmr=True)
+    L = C.lib()
+    ud = torch.from_numpy(ref_to_dev(u0, 2)).to(cuda)
+    t1, t2 = torch.empty_like(ud), torch.empty_like(ud)
+    dt = 0.4 * (1.0 / 60) / (7.0 * 12.0)
+    atol = do.hg_atol()
+    p = lambda x: ctypes.c_void_p(x.data_ptr())  # noqa: E731
+    flagged, mismatches, margin = [], 0, math.inf
+    t = 0.0
+    for step in range(200):
+        for stage, (u_n, u_in, u_out) in enumerate(((None, ud, t1), (ud, t1, t2),
+                                                    (ud, t2, ud)), start=1):
+            alpha, flags = solver.indicator(u_in)
+            torch.cuda.synchronize()
+            uh = dev_to_ref(u_in.cpu().numpy(), cells)
+            a_r = alpha_ref_to_dev(rc.alpha(uh))
+            f_r = a_r > atol
+            f_d = flags.cpu().numpy().astype(bool)
+            mismatches += int(np.count_nonzero(f_d != f_r))
+            flagged.append(int(f_r.sum()))
+            assert np.max(np.abs(alpha.cpu().numpy() - a_r)) <= 1e-14
+            if step % 20 == 0:
+                raw = do.hg_alpha(s, uh, raw=True)
+                margin = min(margin, float(np.min(np.abs(raw - s.alpha_min))))
+            C.check(L.dgsem_ssprk3_stage(solver.handle, stage, p(u_n) if u_n is not None else None,
+                                         p(u_in), p(u_out), t, dt), "stage")
+        t += dt
+    C.check(L.dgsem_check_finite(solver.handle), "finite")
+    print(f"\nDMR 240x60: flagged per stage min/median/max = {min(flagged)}/"
+          f"{int(np.median(flagged))}/{max(flagged)} of {240 * 60}, flag mismatches "
+          f"{mismatches}, min |alpha_raw - alpha_min| = {margin:.3e}")
+    assert mismatches == 0
+    assert max(flagged) > 100  # the shock is developed and flagged
+    u200 = dev_to_ref(ud.cpu().numpy(), cells)
+    du_r = rc.rhs(u200, t)
+    for v in range(5):
+        solver.set_launch_variant(v)
+        err = rel_linf(_rhs(solver, ud, t), du_r)
+        assert err <= RTOL, (v, err)
+
+
+@pytest.mark.parametrize("case", ["kh_hg", "dmr"])
+@pytest.mark.parametrize("vf", ["ranocha", "kennedy_gruber"])
+@pytest.mark.parametrize("sf", ["llf", "hllc"])
+def test_other_fluxes_shock_capturing_match_reference(case, vf, sf, cuda):
+    import torch
+    _need_ref()
+    c = CASES[case]
+    s = do.Scheme(ndims=2, polydeg=3, cells=c["cells"], left=c["left"], right=c["right"],
+                  periodic=c.get("periodic", True), bc=c.get("bc", "periodic"),
+                  shock_capturing=True, volume_flux=vf, surface_flux=sf)
+    u = do.initial_state(s, c["ic"])
+    if c.get("noise"):
+        u = u * (1.0 + c["noise"] * np.random.default_rng(0).standard_normal(u.shape))
+    kind = rb.EULER2D_DMR_HG if case == "dmr" else rb.EULER2D_PERIODIC_HG
+    rc = rb.RefCase(kind, 3, c["cells"], c["left"], c["right"], volume_flux=VFC[vf],
+                    surface_flux=SFC[sf])
+    du_r = rc.rhs(u, 0.011)
+    solver = _solver(2, 3, c["cells"], c["left"], c["right"], vf, sf, hg=True,
+                     dmr=(case == "dmr"))
+    ud = torch.from_numpy(ref_to_dev(u, 2)).to(cuda)
+    for v in range(5):
+        solver.set_launch_variant(v)
+        err = rel_linf(_rhs(solver, ud, 0.011), du_r)
+        assert err <= RTOL, (v, err)
+
+
+@pytest.mark.parametrize("vf", ["ranocha", "kennedy_gruber"])
+def test_other_fluxes_3d_match_reference(vf, cuda):
+    import torch
+    _need_ref()
+    c = CASES["tgv"]
+    s = do.Scheme(ndims=3, polydeg=3, cells=c["cells"], left=c["left"], right=c["right"],
+                  volume_flux=vf)
+    u = do.initial_state(s, "tgv3d")
+    u = u * (1.0 + 0.01 * np.random.default_rng(1).standard_normal(u.shape))
+    rc = rb.RefCase(rb.EULER3D_PERIODIC_SPLIT, 3, c["cells"], c["left"], c["right"],
+                    volume_flux=VFC[vf])
+    du_r = rc.rhs(u, 0.0)
+    solver = _solver(3, 3, c["cells"], c["left"], c["right"], vf, "llf")
+    ud = torch.from_numpy(ref_to_dev(u, 3)).to(cuda)
+    for v in range(6):
+        solver.set_launch_variant(v)
+        err = rel_linf(_rhs(solver, ud, 0.0), du_r)
+        assert err <= RTOL, (v, err)

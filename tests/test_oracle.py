@@ -193,3 +193,55 @@ def test_tangent_linear_reference_value_and_tangent(name):
     h = 1.0e-9
     fd = (ref.rhs(u + h * d, t) - ref.rhs(u - h * d, t)) / (2.0 * h)
     assert np.max(np.abs(fd - dr)) <= 1e-5 * np.max(np.abs(dr))
+
+
+# --------------------------------------------------------------------------
+# Kennedy-Gruber known-answer vectors (C. A. Kennedy, A. Gruber, J. Comput.
+# Phys. 227 (2008), eq. for the split convective flux with arithmetic means):
+#   f_rho = {{rho}} {{v.n}},  f_m = f_rho {{v}} + {{p}} n,
+#   f_E = ({{rho}} {{e}} + {{p}}) {{v.n}},  e = E / rho,
+# evaluated in exact rational arithmetic on rational states (gamma = 7/5).
+# --------------------------------------------------------------------------
+def _kg_exact(primL, primR, normal, gamma):
+    from fractions import Fraction as F
+    nd = len(normal)
+
+    def cons(prim):
+        rho, v, p = prim[0], prim[1:1 + nd], prim[1 + nd]
+        E = p / (gamma - 1) + F(1, 2) * rho * sum(x * x for x in v)
+        return rho, v, p, E / rho
+
+    rL, vL, pL, eL = cons(primL)
+    rR, vR, pR, eR = cons(primR)
+    half = F(1, 2)
+    rho_a, e_a, p_a = half * (rL + rR), half * (eL + eR), half * (pL + pR)
+    va = [half * (vL[d] + vR[d]) for d in range(nd)]
+    vn = sum(va[d] * normal[d] for d in range(nd))
+    f1 = rho_a * vn
+    return [f1] + [f1 * va[d] + p_a * normal[d] for d in range(nd)] + [(rho_a * e_a + p_a) * vn]
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_kennedy_gruber_known_answer(nd):
+    from fractions import Fraction as F
+    gamma = F(7, 5)
+    if nd == 2:
+        primL = [F(1), F(1, 2), F(-1, 4), F(1)]
+        primR = [F(2), F(-1, 2), F(1), F(3, 2)]
+        normal = [F(3, 4), F(-1, 8)]
+    else:
+        primL = [F(1), F(1, 2), F(-1, 4), F(3, 8), F(1)]
+        primR = [F(5, 4), F(-1, 2), F(1), F(-1, 16), F(3, 2)]
+        normal = [F(3, 4), F(-1, 8), F(1, 2)]
+    exact = [float(x) for x in _kg_exact(primL, primR, normal, gamma)]
+    uL = np.array(do.prim_to_cons([np.array([float(x)]) for x in primL], 1.4))
+    uR = np.array(do.prim_to_cons([np.array([float(x)]) for x in primR], 1.4))
+    n = np.array([[float(x)] for x in normal])
+    got = do.flux_kennedy_gruber(uL, uR, n, 1.4)[:, 0]
+    scale = max(abs(x) for x in exact)
+    assert np.max(np.abs(got - np.array(exact))) <= 4e-16 * scale, (got, exact)
+    # the 2D vector worked by hand: {{rho}} = 3/2, {{v}} = (0, 3/8), {{p}} = 5/4,
+    # {{v.n}} = -3/64, e_L = 85/32, e_R = 5/2, {{e}} = 165/64
+    if nd == 2:
+        assert _kg_exact(primL, primR, normal, gamma) == [
+            F(-9, 128), F(15, 16), F(-187, 1024), F(-1965, 8192)]
