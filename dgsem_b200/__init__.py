@@ -15,3 +15,4 @@ from .solver import (  # noqa: F401
     VolumeIntegralShockCapturingHG, VolumeIntegralSplitForm,
 )
 from .solver import Adjoint, BatchGraph, BatchSolver  # noqa: F401,E402
+from .solver import VTUOutputObserver, read_checkpoint, write_checkpoint  # noqa: F401,E402

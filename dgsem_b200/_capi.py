@@ -47,7 +47,9 @@ EXPORTED = [
     "dgsem_batch_autotune", "dgsem_ssprk3_step_static_scratch",
     "dgsem_adjoint_create", "dgsem_adjoint_destroy", "dgsem_adjoint_rhs_vjp",
     "dgsem_kinetic_energy", "dgsem_adjoint_gradient", "dgsem_coordinates_host",
-    "dgsem_fp64_fma_peak",
+    "dgsem_fp64_fma_peak", "dgsem_write_vtu", "dgsem_write_vtu_host",
+    "dgsem_checkpoint_write", "dgsem_checkpoint_read", "dgsem_checkpoint_write_host",
+    "dgsem_checkpoint_read_host",
 ]
 
 
@@ -135,6 +137,15 @@ def lib() -> ctypes.CDLL:
     L.dgsem_adjoint_gradient.argtypes = [vp, dp, c.c_double, c.c_double,
                                          c.POINTER(c.c_double), dp]
     L.dgsem_fp64_fma_peak.argtypes = [vp, c.c_int, c.POINTER(c.c_double), c.POINTER(c.c_double)]
+    L.dgsem_write_vtu.argtypes = [vp, dp, c.c_char_p]
+    L.dgsem_write_vtu_host.argtypes = [c.POINTER(MeshDesc), c.c_double, vp, c.c_char_p]
+    L.dgsem_checkpoint_write.argtypes = [vp, dp, c.c_double, c.c_int64, c.c_char_p]
+    L.dgsem_checkpoint_read.argtypes = [vp, dp, c.POINTER(c.c_double), c.POINTER(c.c_int64),
+                                        c.c_char_p]
+    L.dgsem_checkpoint_write_host.argtypes = [c.POINTER(MeshDesc), c.POINTER(SchemeDesc), vp,
+                                              c.c_double, c.c_int64, c.c_char_p]
+    L.dgsem_checkpoint_read_host.argtypes = [c.POINTER(MeshDesc), vp, c.POINTER(c.c_double),
+                                             c.POINTER(c.c_int64), c.c_char_p]
     for name in EXPORTED:
         f = getattr(L, name)
         if name != "dgsem_status_string":

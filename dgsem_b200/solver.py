@@ -390,10 +390,20 @@ class SSPRK3:
             self.iter += 1
 
     def solve(self, solver: StructuredSolver, sol: Solution, dt: float) -> None:
-        """integrator_base.hpp:21-40: fixed dt until final_time, NaN stops."""
-        while self.time < self.final_time:
+        """integrator_base.hpp:21-40: fixed dt until final_time, NaN stops.
+
+        Observers are objects with the reference's on_step(step, time) ->
+        stop flag and on_finish(step, time) (observer/observer_base.hpp:4-9),
+        or plain callables obs(step, time, sol)."""
+        stop = False
+        while self.time < self.final_time and not stop:
             for obs in self.observers:
-                obs(self.iter, self.time, sol)
+                if hasattr(obs, "on_step"):
+                    stop = bool(obs.on_step(self.iter, self.time)) or stop
+                else:
+                    obs(self.iter, self.time, sol)
+            if stop:
+                break
             self.step(solver, sol, dt)
             self.time += dt
             self.iter += 1
@@ -402,6 +412,63 @@ class SSPRK3:
             except C.DgsemError:
                 self.has_nan = True
                 break
+        for obs in self.observers:
+            if hasattr(obs, "on_finish"):
+                obs.on_finish(self.iter, self.time)
+
+
+# ---------------------------------------------------------------- output
+class VTUOutputObserver:
+    """VTUOutputObserver (observer/vtu_output_observer.hpp:17-235) without VTK:
+    writes <output_path>_step<step>.vtu at step 0, every output_interval
+    steps (never when it is negative) and at the end if the last step was not
+    written; Lagrange cells, point data rho, momentum, rhoE, pressure
+    (dgsem_write_vtu)."""
+
+    def __init__(self, output_path: str, solver: StructuredSolver, sol: Solution,
+                 output_interval: int = -1):
+        self.output_path, self.solver, self.sol = output_path, solver, sol
+        self.output_interval = output_interval
+        self.last_written_step = -1
+        self.written = []
+
+    def filename(self, step: int) -> str:
+        return f"{self.output_path}_step{step}.vtu"
+
+    def write(self, step: int) -> None:
+        torch.cuda.synchronize()
+        name = self.filename(step)
+        C.check(C.lib().dgsem_write_vtu(self.solver.handle, _ptr(self.sol.u), name.encode()),
+                "dgsem_write_vtu")
+        self.last_written_step = step
+        self.written.append(name)
+
+    def on_step(self, step: int, time: float) -> bool:
+        if step == 0 or (self.output_interval > 0 and step % self.output_interval == 0):
+            if step != self.last_written_step:
+                self.write(step)
+        return False
+
+    def on_finish(self, step: int, time: float) -> None:
+        if step != self.last_written_step:
+            self.write(step)
+
+
+def write_checkpoint(path: str, solver: StructuredSolver, sol: Solution, time: float,
+                     step: int) -> None:
+    """Binary checkpoint of the state, time and step (dgsem_checkpoint_write)."""
+    torch.cuda.synchronize()
+    C.check(C.lib().dgsem_checkpoint_write(solver.handle, _ptr(sol.u), float(time), int(step),
+                                           path.encode()), "dgsem_checkpoint_write")
+
+
+def read_checkpoint(path: str, solver: StructuredSolver, sol: Solution):
+    """Restores the state from a checkpoint of the same mesh; returns (time, step)."""
+    t, k = ctypes.c_double(), ctypes.c_int64()
+    C.check(C.lib().dgsem_checkpoint_read(solver.handle, _ptr(sol.u), ctypes.byref(t),
+                                          ctypes.byref(k), path.encode()),
+            "dgsem_checkpoint_read")
+    return t.value, k.value
 
 
 # ---------------------------------------------------------------- discrete adjoint

@@ -347,6 +347,38 @@ dgsem_status dgsem_adjoint_gradient(dgsem_adjoint* adj, const double* u0,
 dgsem_status dgsem_fp64_fma_peak(void* stream, int iters, double* flops_per_s,
                                  double* ms);
 
+/* ---------------------------------------------------------------------------
+ * On-disk output without VTK.
+ * VTU: replaces VTUOutputObserver::write_vtu (observer/vtu_output_observer.hpp:
+ * 65-235) and write_vtu_lagrange_quad/hex (vtu_output_observer_impl.cpp:
+ * 15-117): VTK XML UnstructuredGrid, one Lagrange quadrilateral (2D, cell type
+ * 70) or hexahedron (3D, 72) of order N per element with its nodes in VTK's
+ * Lagrange point order, point data rho, rhou, rhov[, rhow], rhoE, pressure
+ * (pressure with the given / the context's gamma), appended raw binary data.
+ * The device variant copies u (device layout) to the host and synchronises.
+ * The host variant needs no GPU.
+ * ------------------------------------------------------------------------- */
+dgsem_status dgsem_write_vtu(dgsem_ctx* ctx, const double* u, const char* path);
+dgsem_status dgsem_write_vtu_host(const dgsem_mesh_desc* mesh, double gamma,
+                                  const double* u_host, const char* path);
+
+/* Binary checkpoint / restart (no reference counterpart: the reference has no
+ * restart): header (magic "DGSEMCKP", version, mesh and scheme descriptors,
+ * time, step, state length) + the state in the device layout.  Reading
+ * requires the same mesh (degree, cells, domain) and returns
+ * DGSEM_ERR_INVALID_ARG otherwise.  Device variants copy through the host and
+ * synchronise; host variants need no GPU. */
+dgsem_status dgsem_checkpoint_write(dgsem_ctx* ctx, const double* u, double time,
+                                    int64_t step, const char* path);
+dgsem_status dgsem_checkpoint_read(dgsem_ctx* ctx, double* u, double* time,
+                                   int64_t* step, const char* path);
+dgsem_status dgsem_checkpoint_write_host(const dgsem_mesh_desc* mesh,
+                                         const dgsem_scheme_desc* scheme,
+                                         const double* u_host, double time,
+                                         int64_t step, const char* path);
+dgsem_status dgsem_checkpoint_read_host(const dgsem_mesh_desc* mesh, double* u_host,
+                                        double* time, int64_t* step, const char* path);
+
 /* Host-side copies of the basis tables (nodes, weights, inv_weights,
  * lhat(-1), lhat(+1), D, Dsplit, Dhat, inverse Legendre Vandermonde; the
  * n x n tables row-major) for polydeg N; out needs 5n + 4n^2 doubles.

@@ -19,6 +19,10 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB_PATH = os.path.join(_HERE, "_ref", "libdgsem_ref.so")
+# the same reference sources built with floating-point contraction on
+# (oracle/Makefile): the reference against itself under a legal change of
+# rounding, used as the conditioning floor of the full-size parity tests
+REF_FMA_LIB_PATH = os.path.join(_HERE, "_ref", "libdgsem_ref_fma.so")
 
 EULER2D_PERIODIC_SPLIT = 0
 EULER2D_PERIODIC_HG = 1
@@ -48,19 +52,22 @@ class _Case(ctypes.Structure):
 
 
 _lib = None
+_libs: dict = {}
 
 
-def available() -> bool:
-    return os.path.exists(REF_LIB_PATH)
+def available(build: str = "exact") -> bool:
+    return os.path.exists(REF_FMA_LIB_PATH if build == "fma" else REF_LIB_PATH)
 
 
-def lib():
+def lib(build: str = "exact"):
+    """The compiled reference: build "exact" (no contraction, the parity
+    reference) or "fma" (contraction on)."""
     global _lib
-    if _lib is None:
-        if not available():
-            raise FileNotFoundError(
-                f"{REF_LIB_PATH} missing: build it with `make -C oracle ref`")
-        L = ctypes.CDLL(REF_LIB_PATH)
+    if build not in _libs:
+        path = REF_FMA_LIB_PATH if build == "fma" else REF_LIB_PATH
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: build it with `make -C oracle ref`")
+        L = ctypes.CDLL(path)
         L.dgsem_ref_create.restype = ctypes.c_void_p
         L.dgsem_ref_create.argtypes = [ctypes.POINTER(_Case)]
         L.dgsem_ref_destroy.argtypes = [ctypes.c_void_p]
@@ -74,8 +81,10 @@ def lib():
         L.dgsem_ref_geometry.argtypes = [ctypes.c_void_p, dp, dp, dp]
         L.dgsem_ref_basis.argtypes = [ctypes.c_int, dp]
         L.dgsem_ref_omp_threads.restype = ctypes.c_int
-        _lib = L
-    return _lib
+        _libs[build] = L
+        if build == "exact":
+            _lib = L
+    return _libs[build]
 
 
 def _ptr(a: np.ndarray):
@@ -116,6 +125,7 @@ class RefCase:
     alpha_min: float = 0.001
     volume_flux: int = 0    # 0 Chandrashekar, 1 Ranocha (plugin), 2 Kennedy-Gruber (plugin)
     surface_flux: int = 0   # 0 Lax-Friedrichs, 1 HLLC 2D (plugin)
+    build: str = "exact"    # "exact" (no contraction) or "fma" (contraction on)
     _h: int = field(default=0, repr=False)
 
     def __post_init__(self):
@@ -135,13 +145,14 @@ class RefCase:
         c.volume_flux = self.volume_flux
         c.surface_flux = self.surface_flux
         self._c = c
-        self._h = lib().dgsem_ref_create(ctypes.byref(c))
+        self._L = lib(self.build)
+        self._h = self._L.dgsem_ref_create(ctypes.byref(c))
         if not self._h:
             raise ValueError("reference harness rejected the case")
 
     def __del__(self):
-        if getattr(self, "_h", 0) and _lib is not None:
-            _lib.dgsem_ref_destroy(self._h)
+        if getattr(self, "_h", 0) and getattr(self, "_L", None) is not None:
+            self._L.dgsem_ref_destroy(self._h)
             self._h = 0
 
     @property
@@ -164,18 +175,18 @@ class RefCase:
         u = np.ascontiguousarray(u, dtype=np.float64)
         assert u.shape == self.state_shape()
         du = np.zeros_like(u)
-        lib().dgsem_ref_rhs(self._h, _ptr(u), _ptr(du), float(t))
+        self._L.dgsem_ref_rhs(self._h, _ptr(u), _ptr(du), float(t))
         return du
 
     def alpha(self, u: np.ndarray) -> np.ndarray:
         u = np.ascontiguousarray(u, dtype=np.float64)
         a = np.zeros(tuple(self.n_cells[:self.ndims]))
-        lib().dgsem_ref_alpha(self._h, _ptr(u), _ptr(a))
+        self._L.dgsem_ref_alpha(self._h, _ptr(u), _ptr(a))
         return a
 
     def ssprk3(self, u: np.ndarray, t0: float, dt: float, nsteps: int) -> np.ndarray:
         u = np.array(u, dtype=np.float64, order="C", copy=True)
-        lib().dgsem_ref_ssprk3(self._h, _ptr(u), float(t0), float(dt), int(nsteps))
+        self._L.dgsem_ref_ssprk3(self._h, _ptr(u), float(t0), float(dt), int(nsteps))
         return u
 
     def geometry(self):
@@ -185,5 +196,5 @@ class RefCase:
         coords = np.zeros(cells + (nn, nd))
         ja = np.zeros(cells + (nn, nd, nd))
         inv_j = np.zeros(cells + (nn,))
-        lib().dgsem_ref_geometry(self._h, _ptr(coords), _ptr(ja), _ptr(inv_j))
+        self._L.dgsem_ref_geometry(self._h, _ptr(coords), _ptr(ja), _ptr(inv_j))
         return coords, ja, inv_j

