@@ -586,6 +586,23 @@ def run_device_arm(args):
     graph_ms = statistics.mean(a.elapsed_time(b) for a, b in gev)
     L.dgsem_graph_destroy(g)
 
+    # the same steps with the fused diagnostics (volume integrals of kinetic
+    # energy and entropy in the stage-3 epilogue), same flush discipline
+    C.check(L.dgsem_set_diagnostics(h, 1), "diagnostics on")
+    dev_ = [[torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            for _ in range(min(args.steps, 2000))]
+    with torch.cuda.stream(stream):
+        for k, e in enumerate(dev_):
+            flush.fill_(k & 0xFF)
+            step(t, e)
+            t += dt
+        torch.cuda.synchronize()
+    diag_ms = statistics.mean(e[0].elapsed_time(e[3]) for e in dev_)
+    dvol, dke, dent = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    C.check(L.dgsem_diagnostics(h, ctypes.byref(dvol), ctypes.byref(dke), ctypes.byref(dent)),
+            "diagnostics")
+    C.check(L.dgsem_set_diagnostics(h, 0), "diagnostics off")
+
     line = {
         "metric": "FP64 DOF-updates/s per RHS", "value": value, "unit": "DOF-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -608,7 +625,11 @@ def run_device_arm(args):
                     "launch_variant": variant, "variant_ms": variant_ms,
                     "stage_ms_mean": [statistics.mean(x) for x in stage_ms],
                     "step_ms_median": statistics.median(step_ms),
-                    "graph_step_ms_mean": graph_ms, "wall_s_timed_loop": wall},
+                    "graph_step_ms_mean": graph_ms, "wall_s_timed_loop": wall,
+                    "fused_diagnostics": {
+                        "step_ms_mean": diag_ms,
+                        "vs_plain_step": diag_ms / statistics.mean(step_ms),
+                        "mean_kinetic_energy": dke.value, "mean_entropy": dent.value}},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:

@@ -49,7 +49,7 @@ EXPORTED = [
     "dgsem_kinetic_energy", "dgsem_adjoint_gradient", "dgsem_coordinates_host",
     "dgsem_fp64_fma_peak", "dgsem_write_vtu", "dgsem_write_vtu_host",
     "dgsem_checkpoint_write", "dgsem_checkpoint_read", "dgsem_checkpoint_write_host",
-    "dgsem_checkpoint_read_host",
+    "dgsem_checkpoint_read_host", "dgsem_set_diagnostics", "dgsem_diagnostics",
 ]
 
 
@@ -146,6 +146,9 @@ def lib() -> ctypes.CDLL:
                                               c.c_double, c.c_int64, c.c_char_p]
     L.dgsem_checkpoint_read_host.argtypes = [c.POINTER(MeshDesc), vp, c.POINTER(c.c_double),
                                              c.POINTER(c.c_int64), c.c_char_p]
+    L.dgsem_set_diagnostics.argtypes = [vp, c.c_int]
+    L.dgsem_diagnostics.argtypes = [vp, c.POINTER(c.c_double), c.POINTER(c.c_double),
+                                    c.POINTER(c.c_double)]
     for name in EXPORTED:
         f = getattr(L, name)
         if name != "dgsem_status_string":

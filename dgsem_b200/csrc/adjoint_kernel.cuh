@@ -153,7 +153,10 @@ __device__ __forceinline__ void llf_vjp(const FaceState<2>& L, const FaceState<2
   const double vnL = L.v[0] * n[0] + L.v[1] * n[1];
   const double vnR = R.v[0] * n[0] + R.v[1] * n[1];
   const double sn = sqrt(n[0] * n[0] + n[1] * n[1]);
-  const double lam = fmax(fabs(vnL), fabs(vnR)) + fmax(L.a, R.a) * sn;
+  // sound speeds from the squared ones the forward stores; lambda is the
+  // forward's max|v.n| + sqrt(max(a^2) |n|^2) = max|v.n| + max(a) |n|
+  const double aL = sqrt(L.a2), aR = sqrt(R.a2);
+  const double lam = fmax(fabs(vnL), fabs(vnR)) + fmax(aL, aR) * sn;
   const FaceState<2>& O = own_left ? L : R;
   const double vnO = own_left ? vnL : vnR;
   double uo[4] = {0.0, 0.0, 0.0, 0.0};
@@ -171,13 +174,14 @@ __device__ __forceinline__ void llf_vjp(const FaceState<2>& L, const FaceState<2
   const double lamb = -0.5 * (c[0] * (R.u[0] - L.u[0]) + c[1] * (R.u[1] - L.u[1]) +
                               c[2] * (R.u[2] - L.u[2]) + c[3] * (R.u[3] - L.u[3]));
   const bool own_v = own_left ? (fabs(vnL) >= fabs(vnR)) : (fabs(vnR) > fabs(vnL));
-  const bool own_a = own_left ? (L.a >= R.a) : (R.a > L.a);
+  const bool own_a = own_left ? (aL >= aR) : (aR > aL);
+  const double aO = own_left ? aL : aR;
   if (own_v) vnb += lamb * (vnO >= 0.0 ? 1.0 : -1.0);
   double rb = 0.0;
   if (own_a) {
     const double ab = lamb * sn;  // a = sqrt(gamma p / rho)
-    pb += ab * gamma / (2.0 * O.a * O.u[0]);
-    rb += -ab * O.a / (2.0 * O.u[0]);
+    pb += ab * gamma / (2.0 * aO * O.u[0]);
+    rb += -ab * aO / (2.0 * O.u[0]);
   }
   const double vb[2] = {vnb * n[0], vnb * n[1]};
   prim_to_cons_vjp(O.u, gamma - 1.0, rb, vb, pb, uo);

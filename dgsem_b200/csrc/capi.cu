@@ -444,8 +444,11 @@ static dgsem_status launch_stage(dgsem_ctx* ctx, int stage, const double* u_n,
   }
   if (stage > 1 && !u_n) return DGSEM_ERR_INVALID_ARG;
   ctx->launches += ctx->engine->kernels_per_stage();
+  // the stage that completes a step also integrates the new state when the
+  // fused diagnostics are on
+  double* diag = stage == 3 ? ctx->diag_partials : nullptr;
   return cuda_status(ctx->engine->stage(ctx->cfg, u_n, u_in, u_out, a, b, c, ts,
-                                        t_dev, nullptr, stream));
+                                        t_dev, nullptr, stream, diag));
 }
 
 dgsem_status dgsem_ssprk3_stage(dgsem_ctx* ctx, int stage, const double* u_n,
@@ -653,6 +656,66 @@ dgsem_status dgsem_check_finite(dgsem_ctx* ctx) {
     // bit 1: a pipelined stage kernel gave up waiting for a tile copy
     return (h & 2u) ? DGSEM_ERR_TIMEOUT : DGSEM_ERR_NONFINITE;
   }
+  return DGSEM_OK;
+}
+
+namespace {
+// Second pass of the fused diagnostics: the per-block partials summed in a
+// fixed order (each thread a strided subset in index order, then a fixed
+// tree), so the result does not depend on block scheduling.
+__global__ void diag_reduce_kernel(const double* partials, int64_t nslots, double* out) {
+  __shared__ double s[3][256];
+  double a[3] = {0.0, 0.0, 0.0};
+  for (int64_t i = threadIdx.x; i < nslots; i += 256)
+    for (int k = 0; k < 3; ++k) a[k] += partials[3 * i + k];
+  for (int k = 0; k < 3; ++k) s[k][threadIdx.x] = a[k];
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+      for (int k = 0; k < 3; ++k) s[k][threadIdx.x] += s[k][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; ++k) out[k] = s[k][0];
+}
+}  // namespace
+
+dgsem_status dgsem_set_diagnostics(dgsem_ctx* ctx, int enable) {
+  if (!ctx) return DGSEM_ERR_INVALID_ARG;
+  if (!enable) {
+    ctx->diag_partials = nullptr;  // the buffers stay with the context
+    return DGSEM_OK;
+  }
+  if (!ctx->diag_result) {
+    cudaError_t err;
+    // at most one slot per element (every launch shape has >= 1 element per block)
+    double* part = device_alloc<double>(ctx, (size_t)3 * ctx->cfg.nelem, &err);
+    if (!part) return DGSEM_ERR_ALLOC;
+    double* res = device_alloc<double>(ctx, 3, &err);
+    if (!res) return DGSEM_ERR_ALLOC;
+    ctx->diag_result = res;
+    ctx->diag_store = part;
+  }
+  ctx->diag_partials = ctx->diag_store;
+  return DGSEM_OK;
+}
+
+dgsem_status dgsem_diagnostics(dgsem_ctx* ctx, double* volume, double* mean_kinetic_energy,
+                               double* mean_entropy) {
+  if (!ctx || !ctx->diag_partials) return DGSEM_ERR_INVALID_ARG;
+  const int64_t slots = ctx->engine->last_diag_slots();
+  if (slots <= 0) return DGSEM_ERR_INVALID_ARG;  // no step since diagnostics were enabled
+  diag_reduce_kernel<<<1, 256, 0, ctx->stream>>>(ctx->diag_partials, slots, ctx->diag_result);
+  ctx->launches++;
+  double h[3];
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h, ctx->diag_result, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return DGSEM_ERR_CUDA;
+  if (volume) *volume = h[0];
+  if (mean_kinetic_energy) *mean_kinetic_energy = h[1] / h[0];
+  if (mean_entropy) *mean_entropy = h[2] / h[0];
   return DGSEM_OK;
 }
 

@@ -29,6 +29,11 @@ struct dgsem_ctx {
   double* table_block = nullptr;
   unsigned int* flag = nullptr;
   int64_t launches = 0;
+  // fused diagnostics (dgsem_set_diagnostics): per-block partial volume
+  // integrals of the stage-3 output and the reduced (volume, KE, entropy)
+  double* diag_partials = nullptr;  // non-null while enabled
+  double* diag_store = nullptr;
+  double* diag_result = nullptr;
   // failure-path testing: allocation number that fails (0 = none)
   int alloc_calls = 0;
   int fail_alloc_at = 0;

@@ -51,11 +51,15 @@ constexpr int kNumVariants = 6;
 class EngineBase {
  public:
   virtual ~EngineBase() = default;
-  // out = a*u_n + b*u_in + c*RHS(u_in, t); alpha_out optional.
+  // out = a*u_n + b*u_in + c*RHS(u_in, t); alpha_out optional; diag
+  // optional: per-block volume integrals of `out` (StageArgs::diag), as many
+  // slots as diag_slots() returns.
   virtual cudaError_t stage(const EngineConfig& cfg, const double* u_n,
                             const double* u_in, double* out, double a, double b,
                             double c, double t, const double* t_dev,
-                            double* alpha_out, cudaStream_t s) = 0;
+                            double* alpha_out, cudaStream_t s, double* diag = nullptr) = 0;
+  // number of diag slots (blocks) the last stage launch with diag wrote
+  virtual int64_t last_diag_slots() const = 0;
   // Batched launch over a tile list (mesh index and first element per block)
   // of meshes sharing this engine's scheme and degree; per-mesh data in
   // `meshes` (device array).  Tiles are built with elements_per_block().
@@ -90,6 +94,7 @@ inline void fill_basis_const(const BasisTables& b, BasisConst<N>* out) {
       out->Vinv[i][j] = b.Vinv[i][j];
     }
     out->inv_w[i] = b.inv_weights[i];
+    out->w[i] = b.weights[i];
   }
   out->lhat_l0 = b.lhat_left[0];
   out->lhat_rN = b.lhat_right[N - 1];
@@ -199,6 +204,7 @@ class Engine final : public EngineBase {
   void launch_node(const StageArgs<N>& args, int64_t nelem, cudaStream_t s) const {
     if constexpr (kNode) {
       const int64_t blocks = (nelem + NL::EPB - 1) / NL::EPB;
+      last_grid_ = blocks;
       launch_stage_kernel(node_kernel<false, CAP>(), (unsigned)blocks, NL::NT, node_smem(args), s,
                           args);
     }
@@ -236,6 +242,7 @@ class Engine final : public EngineBase {
       }
       const int64_t ntiles = (nelem + NL::EPB - 1) / NL::EPB;
       const int64_t blocks = ntiles < pipe_blocks_ ? ntiles : pipe_blocks_;
+      last_grid_ = blocks;
       launch_stage_kernel(pipe_kernel(), (unsigned)blocks, PSh::NT, PSh::smem_bytes, s, args,
                           (int)ntiles);
     } else {
@@ -292,14 +299,16 @@ class Engine final : public EngineBase {
   void launch(const StageArgs<N>& args, int64_t nelem, cudaStream_t s) const {
     using L = LaunchShape<DIM, N, V>;
     const int64_t blocks = (nelem + L::EPB - 1) / L::EPB;
+    last_grid_ = blocks;
     launch_stage_kernel(kernel<V>(), (unsigned)blocks, L::NT, Sh<V>::smem_bytes, s, args);
   }
 
   cudaError_t stage(const EngineConfig& cfg, const double* u_n,
                     const double* u_in, double* out, double a, double b,
                     double c, double t, const double* t_dev,
-                    double* alpha_out, cudaStream_t s) override {
+                    double* alpha_out, cudaStream_t s, double* diag = nullptr) override {
     StageArgs<N> args = common_args(cfg, a, b, t, t_dev, alpha_out);
+    args.diag = diag;
     args.mesh.u_in = u_in;
     args.mesh.u_n = u_n;
     args.mesh.out = out;
@@ -331,6 +340,7 @@ class Engine final : public EngineBase {
       case 5: launch_pipe(args, cfg.nelem, s); break;
       default: launch<0>(args, cfg.nelem, s); break;
     }
+    if (diag) last_diag_slots_ = last_grid_;
     return cudaGetLastError();
   }
 
@@ -366,6 +376,7 @@ class Engine final : public EngineBase {
   }
 
   int kernels_per_stage() const override { return NS ? 2 : 1; }
+  int64_t last_diag_slots() const override { return last_diag_slots_; }
   int elements_per_block() const override {
     if (variant_ >= 3) return NL::EPB;
     return variant_ == 2 ? LaunchShape<DIM, N, 2>::EPB : LaunchShape<DIM, N, 0>::EPB;
@@ -386,6 +397,8 @@ class Engine final : public EngineBase {
  private:
   int variant_ = 0;
   mutable int64_t pipe_blocks_ = 0;
+  mutable int64_t last_grid_ = 0;  // blocks of the last single-mesh stage launch
+  int64_t last_diag_slots_ = 0;
 };
 
 }  // namespace dgsem

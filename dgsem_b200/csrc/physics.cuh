@@ -170,7 +170,7 @@ struct FaceState {
   double u[DIM + 2];
   double v[DIM];
   double p;
-  double a;  // sound speed
+  double a2;  // squared sound speed gamma p / rho
 };
 
 // (L, R) = first ? (a, b) : (b, a), field by field with selects, so that
@@ -191,8 +191,8 @@ __device__ __forceinline__ void order_states(bool first, const FaceState<DIM>& a
   }
   L.p = first ? a.p : b.p;
   R.p = first ? b.p : a.p;
-  L.a = first ? a.a : b.a;
-  R.a = first ? b.a : a.a;
+  L.a2 = first ? a.a2 : b.a2;
+  R.a2 = first ? b.a2 : a.a2;
 }
 
 template <int DIM>
@@ -209,12 +209,15 @@ __device__ __forceinline__ FaceState<DIM> prepare_face(const double* u,
     sq += s.v[d] * s.v[d];
   }
   s.p = (gamma - 1.0) * (u[DIM + 1] - 0.5 * u[0] * sq);
-  s.a = sqrt(gamma * s.p * inv_rho);
+  s.a2 = gamma * s.p * inv_rho;
   return s;
 }
 
 // Local Lax-Friedrichs flux (numerical_flux.hpp:198-228 with the wave speed
-// of compressible_euler2D.hpp:70-109): 0.5 (F_L + F_R).n - 0.5 lambda (uR-uL).
+// of compressible_euler2D.hpp:70-109): 0.5 (F_L + F_R).n - 0.5 lambda (uR-uL),
+// lambda = max|v.n| + max(a_L, a_R) |n|, evaluated as
+// max|v.n| + sqrt(max(a_L^2, a_R^2) |n|^2): the same value (to rounding) with
+// one square root per evaluation instead of three (two sound speeds, |n|).
 template <int DIM>
 __device__ __forceinline__ void llf_flux(const FaceState<DIM>& L,
                                          const FaceState<DIM>& R,
@@ -226,8 +229,7 @@ __device__ __forceinline__ void llf_flux(const FaceState<DIM>& L,
     vnR += R.v[d] * n[d];
     nn += n[d] * n[d];
   }
-  const double lam =
-      fmax(fabs(vnL), fabs(vnR)) + fmax(L.a, R.a) * sqrt(nn);
+  const double lam = fmax(fabs(vnL), fabs(vnR)) + sqrt(fmax(L.a2, R.a2) * nn);
   f[0] = 0.5 * (L.u[0] * vnL + R.u[0] * vnR) - 0.5 * lam * (R.u[0] - L.u[0]);
 #pragma unroll
   for (int d = 0; d < DIM; ++d) {

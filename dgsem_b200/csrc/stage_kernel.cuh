@@ -40,6 +40,7 @@ struct BasisConst {
   double Dhat[N][N];
   double Vinv[N][N];
   double inv_w[N];
+  double w[N];     // quadrature weights (fused diagnostics)
   double lhat_l0;  // l_0(-1) / w_0
   double lhat_rN;  // l_N(+1) / w_N
 };
@@ -105,7 +106,64 @@ struct StageArgs {
   // runs out with nothing in flight.
   unsigned long long wait_limit_ns;
   int skip_tile_copy;
+  // Fused diagnostics: when non-null, every block writes the volume
+  // integrals (volume, kinetic energy, entropy) of the nodes it stores to
+  // diag[3 * slot] (slot = block, or tile of a persistent launch).
+  double* diag;
 };
+
+// ---------------------------------------------------------------------------
+// Fused per-step diagnostics (analyzer/volume_average_euler.hpp:29-53 with the
+// weights of analyzer/volume_weighted_analyzer_functor.hpp:80,104): for one
+// node of the output state, volume weight w = (w_i w_j [w_k]) / |1/J|,
+// kinetic energy density |m|^2 / (2 rho), entropy density
+// -rho (ln p - gamma ln rho) / (gamma - 1).
+// ---------------------------------------------------------------------------
+template <int DIM, int N>
+__device__ __forceinline__ void diag_add_node(const double* val, const BasisConst<N>& B, int node,
+                                              double inv_j, double gamma, double* acc) {
+  constexpr int NV = DIM + 2;
+  const int in = node % N, jn = (node / N) % N, kn = node / (N * N);
+  double wq = B.w[in] * B.w[jn];
+  if (DIM == 3) wq = wq * B.w[kn];
+  const double w = wq / fabs(inv_j);
+  double m2 = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) m2 += val[1 + d] * val[1 + d];
+  const double ke = 0.5 * m2 / val[0];
+  const double p = (gamma - 1.0) * (val[NV - 1] - ke);
+  const double s = -val[0] * (log(p) - gamma * log(val[0])) / (gamma - 1.0);
+  acc[0] += w;
+  acc[1] += w * ke;
+  acc[2] += w * s;
+}
+
+// Sums acc[3] over the block in a fixed order (warp shuffle tree, then the
+// warps in order) and stores the result at out[0..2]; every thread of the
+// block calls it.  `red` is shared scratch of 3 * (NT / 32) doubles.
+template <int NT>
+__device__ __forceinline__ void diag_block_store(double* acc, double* red, double* out) {
+  static_assert(NT % 32 == 0, "whole warps");
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], o);
+  }
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) red[3 * warp + k] = acc[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s[3] = {0.0, 0.0, 0.0};
+    for (int w = 0; w < NT / 32; ++w)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) s[k] += red[3 * w + k];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) out[k] = s[k];
+  }
+}
 
 // ---------------------------------------------------------------------------
 // Element / node index helpers
@@ -508,7 +566,7 @@ __device__ __forceinline__ void element_face_flux(
 #pragma unroll
   for (int d = 0; d < DIM; ++d) so.v[d] = pr_el[d * NDP + opn];
   so.p = pr_el[Q::P * NDP + opn];
-  so.a = sqrt(gamma * so.p / so.u[0]);
+  so.a2 = gamma * so.p / so.u[0];
   element_face_flux_state<DIM, N, VF, SF, NS, NDP>(p, M, so, us_el, wv_el, I, dir, side, line,
                                                    gamma, t_stage, c0, c1, c2, f);
 }
@@ -614,7 +672,7 @@ __device__ __forceinline__ void process_line(const StageArgs<N>& p, const MeshVi
 #pragma unroll
         for (int d = 0; d < DIM; ++d) st.v[d] = P[d * NDP + nm];
         st.p = P[Q::P * NDP + nm];
-        st.a = sqrt(gamma * st.p / st.u[0]);
+        st.a2 = gamma * st.p / st.u[0];
         return st;
       };
       FaceState<DIM> sl = node_state(0);
@@ -868,11 +926,13 @@ __device__ __forceinline__ void stage_body(const StageArgs<N>& p) {
 
   // ---- phase 3: sum of directions, -1/J, SSPRK3 combination, store -------
   bool bad = false;
+  double dacc[3] = {0.0, 0.0, 0.0};
   const int64_t gbase = (int64_t)e0 * NV * ND;
   for (int idx = tid; idx < ne * ND; idx += NT) {
     const int el = idx / ND, node = idx % ND;
     const int pn = padn<N>(node);
     const double mij = pr[(el * NQ + Q::MIJ) * NDP + pn];
+    double vals[NV];
 #pragma unroll
     for (int q = 0; q < NV; ++q) {
       double du = 0.0;
@@ -885,9 +945,14 @@ __device__ __forceinline__ void stage_body(const StageArgs<N>& p) {
       if (p.a != 0.0) val = p.a * M.u_n[gi] + val;
       bad |= !isfinite(val);
       M.out[gi] = val;
+      vals[q] = val;
     }
+    if (p.diag) diag_add_node<DIM, N>(vals, p.basis, node, -mij, gamma, dacc);
   }
   if (bad) atomicOr(p.nonfinite, 1u);
+  if constexpr (!BATCH && NT % 32 == 0) {
+    if (p.diag) diag_block_store<NT>(dacc, dv, p.diag + 3 * (int64_t)blockIdx.x);
+  }
 }
 
 // Fused stage kernel, register allocation left to the compiler.

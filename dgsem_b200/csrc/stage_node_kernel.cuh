@@ -5,7 +5,7 @@
 //
 // Per block: EPB elements, EPB * n^d threads.
 //   0  element info and the coalesced u_in tile (unpadded shared memory);
-//   1  per-node flux data (NodeKernelSlots), sound speed and -1/J;
+//   1  per-node flux data (NodeKernelSlots), squared sound speed and -1/J;
 //   2a face tasks: every (face, face node) of the block's elements computes
 //      its interface / boundary flux f* once into a shared face buffer
 //      (tasks ordered side-major, so a warp's lanes share the face side and
@@ -38,7 +38,7 @@
 namespace dgsem {
 
 // Shared-memory slots per node (the conserved density comes from the tile).
-//   KG / Chandrashekar: V (v/2, DIM), P (p/2), A (sound speed), MIJ (-1/J),
+//   KG / Chandrashekar: V (v/2, DIM), P (p/2), A (squared sound speed), MIJ (-1/J),
 //                       H_RHO (rho/2), X (KG: e/2; Chandrashekar: beta),
 //                       Y (Chandrashekar: |v|^2/4)
 //   Ranocha:            V (v), P (p), A, MIJ
@@ -303,7 +303,7 @@ __device__ __forceinline__ void node_fv_direction(const StageArgs<N>& p, const M
 #pragma unroll
     for (int d = 0; d < DIM; ++d) st.v[d] = g * P[(K::V + d) * NDP + pk];
     st.p = g * P[K::P * NDP + pk];
-    st.a = P[K::A * NDP + pk];
+    st.a2 = P[K::A * NDP + pk];
     return st;
   };
   auto normal = [&](int fi, double* nrm) {
@@ -427,7 +427,7 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   load_element_tile<N, NV, ND, NDP, EPB, NT>(M.u_in + (int64_t)e0 * NV * ND, us, ne, tid);
   __syncthreads();
 
-  // ---- phase 1: node data, sound speed and -1/J --------------------------
+  // ---- phase 1: node data, squared sound speed and -1/J ------------------
   const int el = tid / ND, node = tid % ND;
   const bool active = el < ne;
   const int pn = padn<N, S::PAD>(node);
@@ -441,7 +441,7 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
 #pragma unroll
     for (int d = 0; d < DIM; ++d) P[(K::V + d) * NDP] = h * s.v[d];
     P[K::P * NDP] = h * s.p;
-    P[K::A * NDP] = sqrt(gamma * s.p / u[0]);
+    P[K::A * NDP] = gamma * s.p / u[0];
     if constexpr (K::HALF) {
       P[K::H_RHO * NDP] = 0.5 * u[0];
       P[K::X * NDP] = VF == VF_KENNEDY_GRUBER ? 0.5 * s.beta : s.beta;
@@ -521,7 +521,7 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
 #pragma unroll
     for (int d = 0; d < DIM; ++d) so.v[d] = g * P[(K::V + d) * NDP + opn];
     so.p = g * P[K::P * NDP + opn];
-    so.a = P[K::A * NDP + opn];
+    so.a2 = P[K::A * NDP + opn];
     double f[NV];
     element_face_flux_state<DIM, N, VF, SF, false, NDP>(p, M, so, U, nullptr, I, dir, side, fn,
                                                         gamma, t_stage, c0, c1, c2, f);
@@ -577,7 +577,11 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
     if (tid == 0) atomicOr(p.nonfinite, 2u);
     return;
   }
-  if (!active) return;
+  // fused diagnostics need every thread of the block for the reduction
+  const bool diag = !BATCH && p.diag != nullptr && NT % 32 == 0;
+  if (!active && !diag) return;
+  double dacc[3] = {0.0, 0.0, 0.0};
+  if (active) {
 
   // ---- phase 3: lifting (surface_integral.hpp:35-154), -1/J, SSPRK3 --------
   {
@@ -602,6 +606,7 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   const double mij = pr[(el * NQ + K::MIJ) * NDP + pn];
   const int64_t gbase = (int64_t)(e0 + el) * NV * ND + node;
   bool bad = false;
+  double vals[NV];
 #pragma unroll
   for (int q = 0; q < NV; ++q) {
     const double du = acc[q] * mij;
@@ -612,8 +617,18 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
       val = p.a * (bulk_n ? stage_n[(el * NV + q) * ND + node] : M.u_n[gi]) + val;
     bad |= !isfinite(val);
     M.out[gi] = val;
+    vals[q] = val;
   }
   if (bad) atomicOr(p.nonfinite, 1u);
+  if (diag) diag_add_node<DIM, N>(vals, p.basis, node, -mij, gamma, dacc);
+  }  // active
+  if constexpr (NT % 32 == 0) {
+    // the face buffer is free after the lifting (3 * NT / 32 doubles)
+    if (diag) {
+      __syncthreads();
+      diag_block_store<NT>(dacc, sf, p.diag + 3 * (int64_t)blockIdx.x);
+    }
+  }
 }
 
 template <int DIM, int N, int VF, int SF, int EPB, bool BATCH, bool HG = false>

@@ -90,6 +90,7 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
   const int el = tid / ND, node = tid % ND;
   const int pn = padn<N, S::B::PAD>(node);
   uint32_t phase = 0;
+  double dacc[3] = {0.0, 0.0, 0.0};  // fused diagnostics of this block's tiles
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x, phase ^= 1u) {
     const int e0 = t * EPB;
     const int ne = min(EPB, nelem - e0);
@@ -139,7 +140,7 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
       return;
     }
 
-    // ---- phase 1: tile -> shared tile + node data, sound speed, -1/J -------
+    // ---- phase 1: tile -> shared tile + node data, a^2, -1/J --------------
     if (active) {
       double u[NV];
 #pragma unroll
@@ -153,7 +154,7 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
 #pragma unroll
       for (int d = 0; d < DIM; ++d) P[(K::V + d) * NDP] = h * s.v[d];
       P[K::P * NDP] = h * s.p;
-      P[K::A * NDP] = sqrt(gamma * s.p / u[0]);
+      P[K::A * NDP] = gamma * s.p / u[0];
       if constexpr (K::HALF) {
         P[K::H_RHO * NDP] = 0.5 * u[0];
         P[K::X * NDP] = VF == VF_KENNEDY_GRUBER ? 0.5 * s.beta : s.beta;
@@ -196,7 +197,7 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
 #pragma unroll
       for (int d = 0; d < DIM; ++d) so.v[d] = g * P[(K::V + d) * NDP + opn];
       so.p = g * P[K::P * NDP + opn];
-      so.a = P[K::A * NDP + opn];
+      so.a2 = P[K::A * NDP + opn];
       double f[NV];
       element_face_flux_state<DIM, N, VF, SF, false, NDP>(p, M, so, U, nullptr, I, dir, side, fn,
                                                           gamma, t_stage, c0, c1, c2, f);
@@ -256,6 +257,7 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
       const double mij = pr[(el * NQ + K::MIJ) * NDP + pn];
       const int64_t gbase = (int64_t)(e0 + el) * NV * ND + node;
       bool bad = false;
+      double vals[NV];
 #pragma unroll
       for (int q = 0; q < NV; ++q) {
         const double du = acc[q] * mij;
@@ -264,13 +266,19 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
         if (with_n) val = p.a * stage_n[(el * NV + q) * ND + node] + val;
         bad |= !isfinite(val);
         M.out[gbase + (int64_t)q * ND] = val;
+        vals[q] = val;
       }
       if (bad) atomicOr(p.nonfinite, 1u);
+      if (p.diag) diag_add_node<DIM, N>(vals, p.basis, node, -mij, gamma, dacc);
     }
     __syncthreads();
     // stage_n, shared tile, node data and face buffer are free again
     if (tid == 0 && with_n && t + (int)gridDim.x < ntiles)
       request(&bar_n, stage_n, M.u_n, t + gridDim.x);
+  }
+  // fused diagnostics: one partial per block over all of its tiles
+  if constexpr (NT % 32 == 0) {
+    if (p.diag) diag_block_store<NT>(dacc, sf, p.diag + 3 * (int64_t)blockIdx.x);
   }
 }
 

@@ -298,6 +298,24 @@ dgsem_status dgsem_autotune(dgsem_ctx* ctx, const double* u, int* chosen,
 /* Selects a launch shape; DGSEM_ERR_INVALID_ARG if the scheme lacks it. */
 dgsem_status dgsem_set_launch_variant(dgsem_ctx* ctx, int variant);
 
+/* Fused per-step diagnostics (replaces the reference's AnalysisObserver with
+ * VolumeAverageEuler, observer/analysis_observer.hpp:56-110,
+ * analyzer/volume_average_euler.hpp:9-69, which re-read the state in a
+ * separate reduction every analysed step): while enabled, the stage-3 launch
+ * of every step (dgsem_ssprk3_stage 3, dgsem_ssprk3_step, graphs captured
+ * while enabled) also integrates the state it writes over the mesh, block by
+ * block: volume sum w, kinetic energy sum w |m|^2/(2 rho), entropy sum
+ * w (-rho (ln p - gamma ln rho) / (gamma - 1)), w = quadrature weight / |1/J|
+ * (volume_weighted_analyzer_functor.hpp:80,104).  Enabling allocates the
+ * partial buffer once (3 doubles per element; call it outside stream
+ * capture).  dgsem_diagnostics sums the partials of the last such launch in a
+ * fixed order (deterministic), returns the volume and the volume means of
+ * kinetic energy and entropy, and synchronises the stream.  The non-finite
+ * check of every stage is dgsem_check_finite. */
+dgsem_status dgsem_set_diagnostics(dgsem_ctx* ctx, int enable);
+dgsem_status dgsem_diagnostics(dgsem_ctx* ctx, double* volume,
+                               double* mean_kinetic_energy, double* mean_entropy);
+
 /* Number of kernel launches issued by this context so far (diagnostics). */
 dgsem_status dgsem_launch_count(const dgsem_ctx* ctx, int64_t* count);
 

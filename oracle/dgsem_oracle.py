@@ -1186,6 +1186,30 @@ def initial_state(s: Scheme, kind: str, **kw):
     return np.stack(cons, axis=-1)
 
 
+def volume_averages(s: Scheme, u):
+    """(volume, mean kinetic energy, mean entropy) of VolumeAverageEuler
+    (analyzer/volume_average_euler.hpp:29-69) with the weights w / |1/J|
+    (volume_weighted_analyzer_functor.hpp:80,104); entropy density
+    -rho (ln p - gamma ln rho) / (gamma - 1)."""
+    U = _grid(s, np.asarray(u))
+    w = s.basis.weights
+    nd = s.ndims
+    if nd == 2:
+        W = w[None, :] * w[:, None]
+    else:
+        W = w[None, None, :] * w[None, :, None] * w[:, None, None]
+    IJ = _grid(s, s.geo.inv_j)
+    wt = W / np.abs(IJ)
+    m2 = 0.0
+    for d in range(nd):
+        m2 = m2 + U[..., 1 + d] * U[..., 1 + d]
+    ke = 0.5 * m2 / U[..., 0]
+    p = (s.gamma - 1.0) * (U[..., nd + 1] - ke)
+    ent = -U[..., 0] * (np.log(p) - s.gamma * np.log(U[..., 0])) / (s.gamma - 1.0)
+    vol = float(np.sum(wt))
+    return vol, float(np.sum(wt * ke)) / vol, float(np.sum(wt * ent)) / vol
+
+
 def kinetic_energy_mean(s: Scheme, u):
     """VolumeAverageEuler kinetic energy with weights w/|1/J|
     (analyzer/volume_average_euler.hpp:9-69, volume_weighted_analyzer_functor.hpp:80,104)."""

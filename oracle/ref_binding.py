@@ -30,8 +30,9 @@ EULER2D_DMR_HG = 2
 EULER3D_PERIODIC_SPLIT = 3
 EULER3D_PERIODIC_HG = 4
 NS2D_PERIODIC_SPLIT = 5
+EULER2D_CENTRAL_DIRICHLET = 6  # the reference's CentralFlux + a user DirichletBC (polydeg 3)
 
-_DIMS = {0: 2, 1: 2, 2: 2, 3: 3, 4: 3, 5: 2}
+_DIMS = {0: 2, 1: 2, 2: 2, 3: 3, 4: 3, 5: 2, 6: 2}
 
 
 class _Case(ctypes.Structure):

@@ -43,6 +43,7 @@ enum {
   REF_EULER3D_PERIODIC_SPLIT = 3,  // TGV-like plain split form
   REF_EULER3D_PERIODIC_HG = 4,     // 3D periodic + HG
   REF_NS2D_PERIODIC_SPLIT = 5,     // Navier-Stokes BR1 + split form
+  REF_EULER2D_CENTRAL_DIRICHLET = 6,  // the reference's CentralFlux + user DirichletBC
 };
 
 typedef struct {
@@ -91,6 +92,19 @@ struct DmrBoundaryState {
     return dmr_state(c, t, gamma);
   }
 };
+// The user Dirichlet state of the plugin-surface test (the same formula as
+// tests/cpp/plugin_central.cu): a density and pressure wave travelling
+// through a uniform flow, conserved variables, gamma = 1.4.
+struct TravellingWave {
+  std::array<T, 4> operator()(const std::array<T, 2>& x, T t) const {
+    const T pi = static_cast<T>(3.14159265358979323846);
+    const T rho = T(1) + T(0.2) * std::sin(pi * (x[0] + x[1] - T(0.4) * t));
+    const T u = T(0.3), v = T(-0.2);
+    const T p = T(1) + T(0.1) * std::cos(pi * (x[0] - x[1]));
+    return {rho, rho * u, rho * v, p / T(0.4) + T(0.5) * rho * (u * u + v * v)};
+  }
+};
+
 struct DmrBottomInflow {
   bool operator()(const std::array<T, 2>& c, T) const {
     return c[0] < static_cast<T>(1.0 / 6.0);
@@ -441,6 +455,16 @@ RefCaseBase* make_case_n(const dgsem_ref_case& c) {
           DGSEM::HGIndicator<Basis, E3>>;
       auto b = DGSEM::BoundarySet(P{}, P{}, P{}, P{}, P{}, P{});
       return new RefCase<E3, N, VF, decltype(b), 3>(c, E3{c.gamma}, b, true);
+    }
+    case REF_EULER2D_CENTRAL_DIRICHLET: {
+      if constexpr (N == 3) {
+        TravellingWave w;
+        auto b = DGSEM::BoundarySet(DGSEM::DirichletBC(w), DGSEM::DirichletBC(w),
+                                    DGSEM::DirichletBC(w), DGSEM::DirichletBC(w));
+        using VF = DGSEM::VolumeIntegralSplitForm<Basis, E2, DGSEM::CentralFlux>;
+        return new RefCase<E2, N, VF, decltype(b), 2>(c, E2{c.gamma}, b, false);
+      }
+      return nullptr;
     }
     case REF_NS2D_PERIODIC_SPLIT: {
       using VF = DGSEM::VolumeIntegralSplitForm<Basis, NS2, DGSEM::ChandrashekarFlux>;
