@@ -45,15 +45,18 @@ void conserved_from_primitive(const double* prim, double gamma, double* cons) {
 // auxiliary kernels
 // ---------------------------------------------------------------------------
 
-template <int N>
+template <int N, int DIM = 2>
 __global__ void indicator_kernel(const double* u, int64_t nelem, int ND,
                                  BasisConst<N> basis, double threshold, double s,
                                  double alpha_min, double alpha_max, double atol,
                                  double* alpha, uint8_t* flags) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nelem) return;
-  const double a = hg_alpha_2d<N>(u + e * 4 * ND, ND, basis, threshold, s,
-                                  alpha_min, alpha_max);
+  double a;
+  if constexpr (DIM == 2)
+    a = hg_alpha_2d<N>(u + e * 4 * ND, ND, basis, threshold, s, alpha_min, alpha_max);
+  else
+    a = hg_alpha_3d<N>(u + e * 5 * ND, ND, basis, threshold, s, alpha_min, alpha_max);
   if (alpha) alpha[e] = a;
   if (flags) flags[e] = (fabs(a - 0.0) > atol) ? 1 : 0;
 }
@@ -186,7 +189,6 @@ dgsem_status validate(const dgsem_mesh_desc* m, const dgsem_scheme_desc* s) {
   }
   if (s->surface_flux == DGSEM_SF_HLLC && m->ndims != 2) return DGSEM_ERR_UNSUPPORTED;
   if (s->volume_integral == DGSEM_VI_SHOCK_CAPTURING_HG) {
-    if (m->ndims != 2) return DGSEM_ERR_UNSUPPORTED;
     if (!(s->alpha_min >= 0.0 && s->alpha_max >= 0.0)) return DGSEM_ERR_INVALID_ARG;
   }
   if (s->equation == DGSEM_NAVIER_STOKES_2D) {
@@ -328,9 +330,8 @@ dgsem_status dgsem_ctx_create(const dgsem_mesh_desc* mesh,
     add(mt.jdiag[a]);
     for (int cc = 0; cc < nd; ++cc) add(mt.ja[a][cc]);
   }
-  if (nd == 2)
-    for (int a = 0; a < 2; ++a)
-      for (int cc = 0; cc < 2; ++cc) add(mt.fv[a][cc]);
+  for (int a = 0; a < nd; ++a)
+    for (int cc = 0; cc < nd; ++cc) add(mt.fv[a][cc]);
   cudaError_t err;
   ctx->table_block = device_alloc<double>(ctx, total + 1, &err);
   if (!ctx->table_block) {
@@ -352,9 +353,8 @@ dgsem_status dgsem_ctx_create(const dgsem_mesh_desc* mesh,
     c.tab.jdiag[a] = place(mt.jdiag[a]);
     for (int cc = 0; cc < nd; ++cc) c.tab.ja[a][cc] = place(mt.ja[a][cc]);
   }
-  if (nd == 2)
-    for (int a = 0; a < 2; ++a)
-      for (int cc = 0; cc < 2; ++cc) c.tab.fv[a][cc] = place(mt.fv[a][cc]);
+  for (int a = 0; a < nd; ++a)
+    for (int cc = 0; cc < nd; ++cc) c.tab.fv[a][cc] = place(mt.fv[a][cc]);
   err = cudaMemcpy(ctx->table_block, host.data(), (total + 1) * sizeof(double),
                    cudaMemcpyHostToDevice);
   ctx->tmp1 = device_alloc<double>(ctx, ctx->state_len, &err);
@@ -569,10 +569,28 @@ dgsem_status dgsem_graph_destroy(dgsem_graph* g) {
 dgsem_status dgsem_indicator(dgsem_ctx* ctx, const double* u, double* alpha,
                              uint8_t* flags) {
   if (!ctx || !u) return DGSEM_ERR_INVALID_ARG;
-  if (ctx->cfg.ndims != 2 || ctx->nvars != 4) return DGSEM_ERR_UNSUPPORTED;
+  if (ctx->scheme.equation == DGSEM_NAVIER_STOKES_2D) return DGSEM_ERR_UNSUPPORTED;
   const EngineConfig& c = ctx->cfg;
   const int threads = 128;
   const unsigned blocks = (unsigned)((c.nelem + threads - 1) / threads);
+  if (c.ndims == 3) {
+#define DGSEM_IND3(NN)                                                       \
+  case NN: {                                                                 \
+    BasisConst<NN> b;                                                        \
+    fill_basis_const<NN>(c.basis, &b);                                       \
+    indicator_kernel<NN, 3><<<blocks, threads, 0, ctx->stream>>>(            \
+        u, c.nelem, ctx->nodes, b, c.hg_threshold, c.hg_s, c.alpha_min,      \
+        c.alpha_max, c.atol, alpha, flags);                                  \
+    break;                                                                   \
+  }
+    switch (c.n) {
+      DGSEM_IND3(2) DGSEM_IND3(3) DGSEM_IND3(4) DGSEM_IND3(5)
+      default: return DGSEM_ERR_UNSUPPORTED;
+    }
+#undef DGSEM_IND3
+    ctx->launches++;
+    return cuda_status(cudaGetLastError());
+  }
 #define DGSEM_IND(NN)                                                        \
   case NN: {                                                                 \
     BasisConst<NN> b;                                                        \

@@ -154,6 +154,9 @@ class Engine final : public EngineBase {
  public:
   static constexpr int GRAD_EPB = (128 / (N * N)) > 0 ? (128 / (N * N)) : 1;
   static constexpr bool kBatch = !NS && !HG;
+  // the line-parallel shapes 0-2 carry shock capturing in 2D only; 3D shock
+  // capturing runs on the node-parallel shapes (0-2 then run shape 3)
+  static constexpr bool kLine = !(DIM == 3 && HG);
 
   template <int V>
   using Sh = StageShape<DIM, N, VF, SF, HG, LaunchShape<DIM, N, V>::EPB, NS>;
@@ -177,24 +180,25 @@ class Engine final : public EngineBase {
 
   template <int V>
   static void set_attributes() {
-    cudaFuncSetAttribute(kernel<V>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)Sh<V>::smem_bytes);
+    if constexpr (kLine)
+      cudaFuncSetAttribute(kernel<V>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)Sh<V>::smem_bytes);
     if constexpr (kBatch)
       cudaFuncSetAttribute(batch_kernel<V>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)Sh<V>::smem_bytes);
   }
 
-  // node-parallel shapes: split form with or without shock capturing (not
-  // Navier-Stokes); batched node launches without shock capturing only
-  static constexpr bool kNode = !NS;
+  // node-parallel shapes: split form with shock capturing or with the
+  // Navier-Stokes viscous terms; batched node launches with neither
+  static constexpr bool kNode = true;
   using NL = NodeLaunch<DIM, N>;
-  using NSh = NodeShape<DIM, N, VF, NL::EPB, HG>;
+  using NSh = NodeShape<DIM, N, VF, NL::EPB, HG, NS>;
   template <bool B, bool CAP>
   static auto node_kernel() {
     if constexpr (CAP)
-      return stage_node_kernel_capped<DIM, N, VF, SF, NL::EPB, B, NL::MINB, HG>;
+      return stage_node_kernel_capped<DIM, N, VF, SF, NL::EPB, B, NL::MINB, HG, NS>;
     else
-      return stage_node_kernel<DIM, N, VF, SF, NL::EPB, B, HG>;
+      return stage_node_kernel<DIM, N, VF, SF, NL::EPB, B, HG, NS>;
   }
   // launches without u_n (a == 0) request the smaller shared-memory size
   static size_t node_smem(const StageArgs<N>& args) {
@@ -297,10 +301,14 @@ class Engine final : public EngineBase {
 
   template <int V>
   void launch(const StageArgs<N>& args, int64_t nelem, cudaStream_t s) const {
-    using L = LaunchShape<DIM, N, V>;
-    const int64_t blocks = (nelem + L::EPB - 1) / L::EPB;
-    last_grid_ = blocks;
-    launch_stage_kernel(kernel<V>(), (unsigned)blocks, L::NT, Sh<V>::smem_bytes, s, args);
+    if constexpr (!kLine) {
+      launch_node<true>(args, nelem, s);
+    } else {
+      using L = LaunchShape<DIM, N, V>;
+      const int64_t blocks = (nelem + L::EPB - 1) / L::EPB;
+      last_grid_ = blocks;
+      launch_stage_kernel(kernel<V>(), (unsigned)blocks, L::NT, Sh<V>::smem_bytes, s, args);
+    }
   }
 
   cudaError_t stage(const EngineConfig& cfg, const double* u_n,
@@ -378,15 +386,15 @@ class Engine final : public EngineBase {
   int kernels_per_stage() const override { return NS ? 2 : 1; }
   int64_t last_diag_slots() const override { return last_diag_slots_; }
   int elements_per_block() const override {
-    if (variant_ >= 3) return NL::EPB;
+    if (variant_ >= 3 || !kLine) return NL::EPB;
     return variant_ == 2 ? LaunchShape<DIM, N, 2>::EPB : LaunchShape<DIM, N, 0>::EPB;
   }
   int threads_per_block() const override {
-    if (variant_ >= 3) return NL::NT;
+    if (variant_ >= 3 || !kLine) return NL::NT;
     return variant_ == 2 ? LaunchShape<DIM, N, 2>::NT : LaunchShape<DIM, N, 0>::NT;
   }
   size_t smem_bytes() const override {
-    if (variant_ >= 3) return NSh::smem_bytes;
+    if (variant_ >= 3 || !kLine) return NSh::smem_bytes;
     return variant_ == 2 ? Sh<2>::smem_bytes : Sh<0>::smem_bytes;
   }
   void set_variant(int v) override { variant_ = (v >= 0 && v < num_variants()) ? v : 0; }

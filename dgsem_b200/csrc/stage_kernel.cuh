@@ -49,7 +49,7 @@ struct DeviceTables {
   const double* ja[3][3];  // ja[a][c]: [eidx_c][node]
   const double* jdiag[3];  // [e_a * n + i]
   const double* coord[3];  // [e_a * n + i]
-  const double* fv[2][2];  // 2D FV subcell normals [eidx_c][f * n + line]
+  const double* fv[3][3];  // FV subcell normals [eidx_c][f * n^(d-1) + line]
 };
 
 enum BcKind : int {
@@ -138,30 +138,46 @@ __device__ __forceinline__ void diag_add_node(const double* val, const BasisCons
   acc[2] += w * s;
 }
 
-// Sums acc[3] over the block in a fixed order (warp shuffle tree, then the
-// warps in order) and stores the result at out[0..2]; every thread of the
-// block calls it.  `red` is shared scratch of 3 * (NT / 32) doubles.
+// Sums acc[3] over the block in a fixed order and stores the result at
+// out[0..2]; every thread of the block calls it (the caller makes the
+// scratch free with a barrier first).  Whole warps: a warp shuffle tree,
+// then the warps in order (`red` holds 3 * NT / 32 doubles); otherwise every
+// thread's values in thread order (`red` holds 3 * NT doubles).
 template <int NT>
 __device__ __forceinline__ void diag_block_store(double* acc, double* red, double* out) {
-  static_assert(NT % 32 == 0, "whole warps");
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if constexpr (NT % 32 == 0) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < 3; ++k) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], o);
-  }
-  __syncthreads();
-  if (lane == 0)
+      for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], o);
+    }
+    __syncthreads();
+    if (lane == 0)
 #pragma unroll
-    for (int k = 0; k < 3; ++k) red[3 * warp + k] = acc[k];
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s[3] = {0.0, 0.0, 0.0};
-    for (int w = 0; w < NT / 32; ++w)
+      for (int k = 0; k < 3; ++k) red[3 * warp + k] = acc[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s[3] = {0.0, 0.0, 0.0};
+      for (int w = 0; w < NT / 32; ++w)
 #pragma unroll
-      for (int k = 0; k < 3; ++k) s[k] += red[3 * w + k];
+        for (int k = 0; k < 3; ++k) s[k] += red[3 * w + k];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) out[k] = s[k];
+      for (int k = 0; k < 3; ++k) out[k] = s[k];
+    }
+  } else {
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 3; ++k) red[3 * threadIdx.x + k] = acc[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s[3] = {0.0, 0.0, 0.0};
+      for (int t = 0; t < NT; ++t)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) s[k] += red[3 * t + k];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) out[k] = s[k];
+    }
   }
 }
 
@@ -268,6 +284,19 @@ __device__ __forceinline__ double hg_node_value(double rho, double m1, double m2
   return __dmul_rn(p, rho);
 }
 
+// Indicator variable rho * p of a 3D node with gamma fixed to 1.4
+// (indicator.hpp:187-210).
+__device__ __forceinline__ double hg_node_value_3d(double rho, double m1, double m2, double m3,
+                                                   double E) {
+  const double u_vel = __ddiv_rn(m1, rho);
+  const double v_vel = __ddiv_rn(m2, rho);
+  const double w_vel = __ddiv_rn(m3, rho);
+  const double vv = __dadd_rn(__dadd_rn(__dmul_rn(u_vel, u_vel), __dmul_rn(v_vel, v_vel)),
+                              __dmul_rn(w_vel, w_vel));
+  const double p = __dmul_rn(1.4 - 1.0, __dsub_rn(E, __dmul_rn(__dmul_rn(0.5, rho), vv)));
+  return __dmul_rn(p, rho);
+}
+
 // Modal energies -> logistic alpha with clipping (indicator.hpp:385-416).
 __device__ __forceinline__ double hg_alpha_from_energies(double total, double c1, double c2,
                                                          double threshold, double s,
@@ -305,6 +334,89 @@ __device__ __forceinline__ void hg_energy_sums(const double* m2, double* total, 
   *total = t;
   *c1 = a;
   *c2 = b;
+}
+
+// The 3D energy sums over m2[k*N*N + j*N + i] in the reference's order and
+// coverage (indicator.hpp:494-544): clip2 over i, j, k < N-2; clip1 adds the
+// index-(N-2) layers; total adds the layer k = N-1 and the rows j = N-1 of
+// k < N-1.
+template <int N>
+__device__ __forceinline__ void hg_energy_sums_3d(const double* m2, double* total, double* c1,
+                                                  double* c2) {
+  auto at = [&](int k, int j, int i) { return m2[(k * N + j) * N + i]; };
+  double b = 0.0;
+#pragma unroll
+  for (int k = 0; k + 2 < N; ++k)
+#pragma unroll
+    for (int j = 0; j + 2 < N; ++j)
+#pragma unroll
+      for (int i = 0; i + 2 < N; ++i) b = __dadd_rn(b, at(k, j, i));
+  double a = b;
+  if (N >= 2) {
+#pragma unroll
+    for (int j = 0; j + 1 < N; ++j)
+#pragma unroll
+      for (int i = 0; i + 1 < N; ++i) a = __dadd_rn(a, at(N - 2, j, i));
+#pragma unroll
+    for (int k = 0; k + 2 < N; ++k)
+#pragma unroll
+      for (int i = 0; i + 1 < N; ++i) a = __dadd_rn(a, at(k, N - 2, i));
+#pragma unroll
+    for (int k = 0; k + 2 < N; ++k)
+#pragma unroll
+      for (int j = 0; j + 2 < N; ++j) a = __dadd_rn(a, at(k, j, N - 2));
+  }
+  double t = a;
+#pragma unroll
+  for (int j = 0; j < N; ++j)
+#pragma unroll
+    for (int i = 0; i < N; ++i) t = __dadd_rn(t, at(N - 1, j, i));
+#pragma unroll
+  for (int k = 0; k + 1 < N; ++k)
+#pragma unroll
+    for (int i = 0; i < N; ++i) t = __dadd_rn(t, at(k, N - 1, i));
+  *total = t;
+  *c1 = a;
+  *c2 = b;
+}
+
+// Single-thread 3D indicator (standalone indicator kernel), ND = N^3 the
+// stride between variables: the dimension-wise modal transform
+// (indicator.hpp:69-111) in the reference's order, then the energies.
+template <int N>
+__device__ double hg_alpha_3d(const double* us_el, int ND, const BasisConst<N>& B,
+                              double threshold, double s, double alpha_min, double alpha_max) {
+  double a[N * N * N], b[N * N * N];
+  for (int node = 0; node < N * N * N; ++node)
+    a[node] = hg_node_value_3d(us_el[node], us_el[ND + node], us_el[2 * ND + node],
+                               us_el[3 * ND + node], us_el[4 * ND + node]);
+  for (int k = 0; k < N; ++k)
+    for (int j = 0; j < N; ++j)
+      for (int i = 0; i < N; ++i) {
+        double r = 0.0;
+        for (int ii = 0; ii < N; ++ii)
+          r = __dadd_rn(r, __dmul_rn(B.Vinv[i][ii], a[(k * N + j) * N + ii]));
+        b[(k * N + j) * N + i] = r;
+      }
+  for (int k = 0; k < N; ++k)
+    for (int j = 0; j < N; ++j)
+      for (int i = 0; i < N; ++i) {
+        double r = 0.0;
+        for (int jj = 0; jj < N; ++jj)
+          r = __dadd_rn(r, __dmul_rn(B.Vinv[j][jj], b[(k * N + jj) * N + i]));
+        a[(k * N + j) * N + i] = r;
+      }
+  for (int k = 0; k < N; ++k)
+    for (int j = 0; j < N; ++j)
+      for (int i = 0; i < N; ++i) {
+        double r = 0.0;
+        for (int kk = 0; kk < N; ++kk)
+          r = __dadd_rn(r, __dmul_rn(B.Vinv[k][kk], a[(kk * N + j) * N + i]));
+        b[(k * N + j) * N + i] = __dmul_rn(r, r);
+      }
+  double total, c1, c2;
+  hg_energy_sums_3d<N>(b, &total, &c1, &c2);
+  return hg_alpha_from_energies(total, c1, c2, threshold, s, alpha_min, alpha_max);
 }
 
 // Single-thread version (standalone indicator kernel).  ND is the stride
@@ -950,7 +1062,7 @@ __device__ __forceinline__ void stage_body(const StageArgs<N>& p) {
     if (p.diag) diag_add_node<DIM, N>(vals, p.basis, node, -mij, gamma, dacc);
   }
   if (bad) atomicOr(p.nonfinite, 1u);
-  if constexpr (!BATCH && NT % 32 == 0) {
+  if constexpr (!BATCH) {
     if (p.diag) diag_block_store<NT>(dacc, dv, p.diag + 3 * (int64_t)blockIdx.x);
   }
 }

@@ -56,7 +56,7 @@ struct NodeKernelSlots {
                             : VF == VF_KENNEDY_GRUBER ? DIM + 5 : DIM + 3;
 };
 
-template <int DIM, int N, int VF, int EPB, bool HG = false>
+template <int DIM, int N, int VF, int EPB, bool HG = false, bool NS = false>
 struct NodeShape {
   static constexpr int NV = DIM + 2;
   static constexpr int ND = ipow(N, DIM);
@@ -70,7 +70,7 @@ struct NodeShape {
   static constexpr int SM_P = EPB * NQ * NDP;
   // f* [el][face][fn][var]; with shock capturing also the indicator scratch
   static constexpr int SM_F0 = EPB * NFACE * NF * NV;
-  static constexpr int SM_F = HG && 3 * EPB * ND > SM_F0 ? 3 * EPB * ND : SM_F0;
+  static constexpr int SM_F = HG && 2 * EPB * ND > SM_F0 ? 2 * EPB * ND : SM_F0;
   static constexpr int SM_A = HG ? EPB : 0;        // alpha per element
   static constexpr int SM_VINV = HG ? N * N : 0;   // inverse Legendre Vandermonde
   // volume-term exchange buffer [round][var][thread]: fluxes of the pairs
@@ -87,8 +87,11 @@ struct NodeShape {
   // smem_bytes_base and leave the rest of the SM's storage to L1
   static constexpr int SM_N = (NV * ND) % 2 == 0 ? EPB * NV * ND : 0;
   static constexpr int NT = EPB * ND;
+  // Navier-Stokes: -F_v per node [el][dim][var][node] (2D)
+  static constexpr int SM_W = NS ? EPB * 2 * NV * ND : 0;
   static constexpr size_t smem_bytes_base =
-      sizeof(double) * (SM_U + SM_P + SM_F + SM_A + SM_VINV + SM_X) + sizeof(int) * EPB * NI;
+      sizeof(double) * (SM_U + SM_P + SM_F + SM_A + SM_VINV + SM_X + SM_W) +
+      sizeof(int) * EPB * NI;
   static constexpr size_t off_n_bytes = (smem_bytes_base + 15) / 16 * 16;
   static constexpr size_t smem_bytes = off_n_bytes + sizeof(double) * SM_N;
 };
@@ -281,19 +284,21 @@ __device__ __forceinline__ void node_volume_direction(const StageArgs<N>& p, con
 }
 
 // Hennemann-Gassner FV subcell contribution of direction DIR to the node
-// (volume_flux.hpp:457-509): LLF on the subcell normals at the node's two
-// subcell interfaces, weighted by alpha / w_m (each interface flux is
-// evaluated by both of its nodes).
+// (volume_flux.hpp:457-509 in 2D, :521-630 in 3D): LLF on the subcell normals
+// at the node's two subcell interfaces, weighted by alpha / w_m (each
+// interface flux is evaluated by both of its nodes).
 template <int DIR, int DIM, int N, int VF, int NDP>
 __device__ __forceinline__ void node_fv_direction(const StageArgs<N>& p, const MeshView& M,
                                                   const double* U, const double* P,
                                                   const int* I, int node, double alpha,
                                                   double* acc) {
   constexpr int NV = DIM + 2;
+  constexpr int NF = ipow(N, DIM - 1);
   using K = NodeKernelSlots<DIM, VF>;
-  static_assert(DIM == 2, "shock capturing: 2D");
-  const int m = DIR == 0 ? node % N : node / N;
-  const int line = DIR == 0 ? node / N : node % N;
+  const int m = DIR == 0 ? node % N : DIR == 1 ? (node / N) % N : node / (N * N);
+  const int line = DIR == 0 ? node / N
+                   : DIR == 1 ? node % N + N * (node / (N * N))
+                              : node % (N * N);
   auto state = [&](int k) {
     const int pk = padn<N, (NDP != ipow(N, DIM))>(line_node<DIM, N>(DIR, line, k));
     FaceState<DIM> st;
@@ -309,7 +314,7 @@ __device__ __forceinline__ void node_fv_direction(const StageArgs<N>& p, const M
   auto normal = [&](int fi, double* nrm) {
 #pragma unroll
     for (int c = 0; c < DIM; ++c)
-      nrm[c] = __ldg(M.tab.fv[DIR][c] + (int64_t)I[3 + c] * (N - 1) * N + (fi - 1) * N + line);
+      nrm[c] = __ldg(M.tab.fv[DIR][c] + (int64_t)I[3 + c] * (N - 1) * NF + (fi - 1) * NF + line);
   };
   const double w = alpha * p.basis.inv_w[m];
   const FaceState<DIM> own = state(m);
@@ -332,10 +337,10 @@ __device__ __forceinline__ void node_fv_direction(const StageArgs<N>& p, const M
   }
 }
 
-template <int DIM, int N, int VF, int SF, int EPB, bool BATCH, bool HG>
+template <int DIM, int N, int VF, int SF, int EPB, bool BATCH, bool HG, bool NS = false>
 __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
-  static_assert(!HG || DIM == 2, "shock capturing: 2D only");
-  using S = NodeShape<DIM, N, VF, EPB, HG>;
+  static_assert(!NS || (DIM == 2 && !HG && !BATCH), "Navier-Stokes: 2D split form");
+  using S = NodeShape<DIM, N, VF, EPB, HG, NS>;
   using K = NodeKernelSlots<DIM, VF>;
   constexpr int NV = S::NV, ND = S::ND, NDP = S::NDP, NF = S::NF, NFACE = S::NFACE,
                 NQ = S::NQ, NI = S::NI, NT = S::NT;
@@ -346,7 +351,8 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   double* alpha_s = sf + S::SM_F;          // [el] (shock capturing)
   double* vinv_s = alpha_s + S::SM_A;      // [N][N] (shock capturing)
   double* xbuf = vinv_s + S::SM_VINV;      // volume-term exchange
-  int* info = reinterpret_cast<int*>(xbuf + S::SM_X);
+  double* wv = xbuf + S::SM_X;             // Navier-Stokes -F_v [el][dim][var][node]
+  int* info = reinterpret_cast<int*>(wv + S::SM_W);
   // [el][var][node] u_n tile (bulk-copy target; present when p.a != 0)
   double* stage_n = reinterpret_cast<double*>(reinterpret_cast<char*>(smem_node) + S::off_n_bytes);
 
@@ -456,6 +462,24 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
       jdet = jdet * (__ldg(M.tab.jdiag[1] + I[1] * N + jn) * __ldg(M.tab.jdiag[2] + I[2] * N + kn));
     }
     P[K::MIJ * NDP] = -(1.0 / jdet);
+    if constexpr (NS) {
+      // -F_v at the node from the lifted gradient (parabolic_viscous.hpp:358-396)
+      double q[4], gx[4], gy[4];
+      ns_gradient_variables(u, gamma, q);
+      const double* G = p.grad + (int64_t)(e0 + el) * 4 * 2 * ND + node;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        gx[v] = __ldg(G + (v * 2 + 0) * ND);
+        gy[v] = __ldg(G + (v * 2 + 1) * ND);
+      }
+#pragma unroll
+      for (int d = 0; d < 2; ++d) {
+        double f[4];
+        ns_neg_viscous_flux(q, gx, gy, p.mu, p.kappa, d, f);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) wv[((el * 2 + d) * NV + v) * ND + node] = f[v];
+      }
+    }
   }
   __syncthreads();
 
@@ -464,34 +488,56 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   // stage_kernel.cuh (identical alpha and troubled-cell flags); scratch in the
   // face buffer, which is written only afterwards ------------------------------
   if constexpr (HG) {
-    double* ind = sf;                // [el][ND]
-    double* tmp = sf + EPB * ND;     // [el][ND]
-    double* m2 = sf + 2 * EPB * ND;  // [el][ND]
-    const int ii0 = node % N, jj0 = node / N;
+    // two scratch arrays used in turn: node values (A) -> x pass (B) -> y
+    // pass (A) [-> z pass (B) in 3D]; the last pass stores squared modes
+    double* bufA = sf;             // [el][ND]
+    double* bufB = sf + EPB * ND;  // [el][ND]
+    const int i0 = node % N, j0 = (node / N) % N, k0 = DIM == 3 ? node / (N * N) : 0;
     if (active) {
       const double* Ue = us + el * NV * NDP;
-      ind[el * ND + node] = hg_node_value(Ue[pn], Ue[NDP + pn], Ue[2 * NDP + pn], Ue[3 * NDP + pn]);
+      if constexpr (DIM == 2)
+        bufA[el * ND + node] =
+            hg_node_value(Ue[pn], Ue[NDP + pn], Ue[2 * NDP + pn], Ue[3 * NDP + pn]);
+      else
+        bufA[el * ND + node] = hg_node_value_3d(Ue[pn], Ue[NDP + pn], Ue[2 * NDP + pn],
+                                                Ue[3 * NDP + pn], Ue[4 * NDP + pn]);
     }
     __syncthreads();
-    if (active) {
+    if (active) {  // x: sum_ii V(i, ii) ind(.., ii)
       double r = 0.0;
 #pragma unroll
       for (int ii = 0; ii < N; ++ii)
-        r = __dadd_rn(r, __dmul_rn(vinv_s[ii0 * N + ii], ind[el * ND + jj0 * N + ii]));
-      tmp[el * ND + node] = r;
+        r = __dadd_rn(r, __dmul_rn(vinv_s[i0 * N + ii], bufA[el * ND + node - i0 + ii]));
+      bufB[el * ND + node] = r;
     }
     __syncthreads();
-    if (active) {
+    if (active) {  // y: sum_jj V(j, jj) tmp(.., jj, i)
       double r = 0.0;
 #pragma unroll
       for (int jj = 0; jj < N; ++jj)
-        r = __dadd_rn(r, __dmul_rn(vinv_s[jj0 * N + jj], tmp[el * ND + jj * N + ii0]));
-      m2[el * ND + node] = __dmul_rn(r, r);
+        r = __dadd_rn(r, __dmul_rn(vinv_s[j0 * N + jj],
+                                   bufB[el * ND + node + (jj - j0) * N]));
+      bufA[el * ND + node] = DIM == 2 ? __dmul_rn(r, r) : r;
     }
     __syncthreads();
+    if constexpr (DIM == 3) {
+      if (active) {  // z: sum_kk V(k, kk) tmp(kk, j, i)
+        double r = 0.0;
+#pragma unroll
+        for (int kk = 0; kk < N; ++kk)
+          r = __dadd_rn(r, __dmul_rn(vinv_s[k0 * N + kk],
+                                     bufA[el * ND + node + (kk - k0) * N * N]));
+        bufB[el * ND + node] = __dmul_rn(r, r);
+      }
+      __syncthreads();
+    }
+    double* m2 = DIM == 2 ? bufA : bufB;
     if (tid < ne) {
       double total, c1e, c2e;
-      hg_energy_sums<N>(m2 + tid * ND, &total, &c1e, &c2e);
+      if constexpr (DIM == 2)
+        hg_energy_sums<N>(m2 + tid * ND, &total, &c1e, &c2e);
+      else
+        hg_energy_sums_3d<N>(m2 + tid * ND, &total, &c1e, &c2e);
       const double a = hg_alpha_from_energies(total, c1e, c2e, p.hg_threshold, p.hg_s,
                                               p.alpha_min, p.alpha_max);
       alpha_s[tid] = a;
@@ -523,8 +569,10 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
     so.p = g * P[K::P * NDP + opn];
     so.a2 = P[K::A * NDP + opn];
     double f[NV];
-    element_face_flux_state<DIM, N, VF, SF, false, NDP>(p, M, so, U, nullptr, I, dir, side, fn,
-                                                        gamma, t_stage, c0, c1, c2, f);
+    element_face_flux_state<DIM, N, VF, SF, NS, NDP>(p, M, so, U,
+                                                     NS ? wv + fe * 2 * NV * ND : nullptr, I,
+                                                     dir, side, fn, gamma, t_stage, c0, c1, c2,
+                                                     f);
     double* F = sf + ((fe * NFACE + face) * NF + fn) * NV;
 #pragma unroll
     for (int q = 0; q < NV; ++q) F[q] = f[q];
@@ -554,6 +602,27 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
     if constexpr (DIM == 3)
       node_volume_direction<2, DIM, N, VF, NDP, WARP_ALL, S::XCHG>(p, M, U, P, I, node, pn, own,
                                                                   hgm1, acc, xbuf, tid, NT);
+    if constexpr (NS) {
+      // viscous weak-form volume term sum_k Dhat(m, k) Ja^dir(k) . (-F_v)(k)
+      // along each line through the node (parabolic_viscous.hpp:418-466)
+      const double* W = wv + ev * 2 * NV * ND;
+#pragma unroll
+      for (int dir = 0; dir < 2; ++dir) {
+        const int m = dir == 0 ? node % N : node / N;
+        const int stride = dir == 0 ? 1 : N;
+        const double* j0 = M.tab.ja[dir][0] + (int64_t)I[3] * ND;
+        const double* j1 = M.tab.ja[dir][1] + (int64_t)I[4] * ND;
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+          const int nk = node + (k - m) * stride;
+          const double a0 = __ldg(j0 + nk), a1 = __ldg(j1 + nk);
+          const double dmk = p.basis.Dhat[m][k];
+#pragma unroll
+          for (int q = 0; q < NV; ++q)
+            acc[q] += dmk * (a0 * W[(0 * NV + q) * ND + nk] + a1 * W[(1 * NV + q) * ND + nk]);
+        }
+      }
+    }
   }
   if constexpr (HG) {
     if (active) {
@@ -568,6 +637,8 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
         for (int q = 0; q < NV; ++q) acc[q] *= one_m;
         node_fv_direction<0, DIM, N, VF, NDP>(p, M, U, P, I, node, alpha, acc);
         node_fv_direction<1, DIM, N, VF, NDP>(p, M, U, P, I, node, alpha, acc);
+        if constexpr (DIM == 3)
+          node_fv_direction<2, DIM, N, VF, NDP>(p, M, U, P, I, node, alpha, acc);
       }
     }
   }
@@ -578,7 +649,7 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
     return;
   }
   // fused diagnostics need every thread of the block for the reduction
-  const bool diag = !BATCH && p.diag != nullptr && NT % 32 == 0;
+  const bool diag = !BATCH && p.diag != nullptr;
   if (!active && !diag) return;
   double dacc[3] = {0.0, 0.0, 0.0};
   if (active) {
@@ -622,26 +693,25 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   if (bad) atomicOr(p.nonfinite, 1u);
   if (diag) diag_add_node<DIM, N>(vals, p.basis, node, -mij, gamma, dacc);
   }  // active
-  if constexpr (NT % 32 == 0) {
-    // the face buffer is free after the lifting (3 * NT / 32 doubles)
-    if (diag) {
-      __syncthreads();
-      diag_block_store<NT>(dacc, sf, p.diag + 3 * (int64_t)blockIdx.x);
-    }
+  // the state tile is free after the epilogue (it holds NV * NT >= 3 * NT doubles)
+  if (diag) {
+    __syncthreads();
+    diag_block_store<NT>(dacc, us, p.diag + 3 * (int64_t)blockIdx.x);
   }
 }
 
-template <int DIM, int N, int VF, int SF, int EPB, bool BATCH, bool HG = false>
+template <int DIM, int N, int VF, int SF, int EPB, bool BATCH, bool HG = false, bool NS = false>
 __global__ void __launch_bounds__(EPB* ipow(N, DIM)) stage_node_kernel(const StageArgs<N> p) {
-  stage_node_body<DIM, N, VF, SF, EPB, BATCH, HG>(p);
+  stage_node_body<DIM, N, VF, SF, EPB, BATCH, HG, NS>(p);
 }
 
 // Same kernel with MINB resident blocks per SM requested from the register
 // allocator.
-template <int DIM, int N, int VF, int SF, int EPB, bool BATCH, int MINB, bool HG = false>
+template <int DIM, int N, int VF, int SF, int EPB, bool BATCH, int MINB, bool HG = false,
+          bool NS = false>
 __global__ void __launch_bounds__(EPB* ipow(N, DIM), MINB)
     stage_node_kernel_capped(const StageArgs<N> p) {
-  stage_node_body<DIM, N, VF, SF, EPB, BATCH, HG>(p);
+  stage_node_body<DIM, N, VF, SF, EPB, BATCH, HG, NS>(p);
 }
 
 }  // namespace dgsem

@@ -277,9 +277,8 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
       request(&bar_n, stage_n, M.u_n, t + gridDim.x);
   }
   // fused diagnostics: one partial per block over all of its tiles
-  if constexpr (NT % 32 == 0) {
-    if (p.diag) diag_block_store<NT>(dacc, sf, p.diag + 3 * (int64_t)blockIdx.x);
-  }
+  // the state tile is free after the last tile (NV * NT >= 3 * NT doubles)
+  if (p.diag) diag_block_store<NT>(dacc, us, p.diag + 3 * (int64_t)blockIdx.x);
 }
 
 template <int DIM, int N, int VF, int SF, int EPB, int MINB>

@@ -386,6 +386,33 @@ bool make_metric_tables(const BasisTables& b, int ndims, const int64_t* cells,
             t.ja[a][c][eidx * nd + node] = ja[node * 9 + a * 3 + c];
       }
   }
+  // global_def.hpp:296-440: cumulative subcell normals along each line,
+  // normal_dir(face f) = Ja^dir(node 0) + sum_{f' <= f} sum_m w_f' D(f', m) Ja^dir(node m)
+  const int nf = n * n;
+  for (int dir = 0; dir < 3; ++dir)
+    for (int c = 0; c < 3; ++c) {
+      const int64_t ne = other_axes_count(3, cells, c);
+      std::vector<double>& fv = t.fv[dir][c];
+      fv.assign(ne * (n - 1) * nf, 0.0);
+      const std::vector<double>& JA = t.ja[dir][c];
+      for (int64_t e = 0; e < ne; ++e)
+        for (int line = 0; line < nf; ++line) {
+          auto ja_at = [&](int pos) {
+            const int a = line % n, b2 = line / n;  // the two other node indices
+            const int node = dir == 0 ? pos + n * a + nf * b2
+                             : dir == 1 ? a + n * pos + nf * b2 : a + n * b2 + nf * pos;
+            return JA[e * nd + node];
+          };
+          double acc = ja_at(0);
+          for (int m = 0; m < n; ++m) acc += b.weights[0] * b.D[0][m] * ja_at(m);
+          fv[e * (n - 1) * nf + 0 * nf + line] = acc;
+          for (int f = 1; f < n - 1; ++f) {
+            acc = fv[e * (n - 1) * nf + (f - 1) * nf + line];
+            for (int m = 0; m < n; ++m) acc += b.weights[f] * b.D[f][m] * ja_at(m);
+            fv[e * (n - 1) * nf + f * nf + line] = acc;
+          }
+        }
+    }
   return true;
 }
 

@@ -16,8 +16,8 @@
 //     1/J = 1 / (J00 * J11 [* J22]) because the off-diagonal products of the
 //     reference's determinant are ~eps^2 relative and never change the
 //     rounded result;
-//   * the 2D FV subcell normals (base/global_def.hpp:174-252) are cumulative
-//     sums of Ja along a line and factor the same way.
+//   * the FV subcell normals (base/global_def.hpp:174-252 in 2D, :296-440 in
+//     3D) are cumulative sums of Ja along a line and factor the same way.
 // The tables are computed by restating the reference's loops in the same
 // accumulation order with no FP contraction, so they agree bitwise.
 #pragma once
@@ -56,8 +56,9 @@ struct MetricTablesHost {
   std::vector<double> jdiag[3];
   // ja[a][c][eidx_c * n^d + node]
   std::vector<double> ja[3][3];
-  // 2D FV subcell normals: fv[dir][c][eidx_c * (n-1) * n + f * n + line]
-  std::vector<double> fv[2][2];
+  // FV subcell normals: fv[dir][c][eidx_c * (n-1) * n^(d-1) + f * n^(d-1) + line]
+  // (line = the node index over the axes != dir, first axis fastest)
+  std::vector<double> fv[3][3];
 };
 
 // Element-index of the axes other than c (x fastest):

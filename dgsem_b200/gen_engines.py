@@ -27,10 +27,15 @@ def combos():
         for sf in range(2):
             for hg in range(2):
                 out.add((2, 4, vf, sf, hg))
-    # 3D Euler (periodic): n in 2..5 with the three volume fluxes and LLF.
+    # 3D Euler (periodic): n in 2..5 with the three volume fluxes and LLF, and
+    # Hennemann-Gassner shock capturing with Chandrashekar/LLF; at n = 4 with
+    # every volume flux.
     for n in range(2, 6):
         for vf in range(3):
             out.add((3, n, vf, 0, 0))
+        out.add((3, n, 0, 0, 1))
+    for vf in range(3):
+        out.add((3, 4, vf, 0, 1))
     return sorted((d, n, vf, sf, hg, 0) for (d, n, vf, sf, hg) in out) + ns_combos()
 
 

@@ -402,6 +402,29 @@ RefCaseBase* make_hg_2d(const dgsem_ref_case& c, const DGSEM::equations::Compres
   return make_hg_2d_vf<N, DGSEM::ChandrashekarFlux>(c, eq, b, periodic);
 }
 
+// 3D periodic shock capturing with the volume flux chosen by c.volume_flux
+// (the plugin fluxes at polydeg 3 only).
+template <std::size_t N, template <class> class VFlux>
+RefCaseBase* make_hg_3d_vf(const dgsem_ref_case& c) {
+  using Basis = DGSEM::Basis::LobattoLegendreBasis<T, N>;
+  using E3 = DGSEM::equations::CompressibleEuler3D<T>;
+  using VF = DGSEM::VolumeIntegralShockCapturingHG<Basis, E3, VFlux, DGSEM::LaxFriedrichsFlux,
+                                                   DGSEM::HGIndicator<Basis, E3>>;
+  using P = DGSEM::PeriodicBC;
+  auto b = DGSEM::BoundarySet(P{}, P{}, P{}, P{}, P{}, P{});
+  return new RefCase<E3, N, VF, decltype(b), 3>(c, E3{c.gamma}, b, true);
+}
+
+template <std::size_t N>
+RefCaseBase* make_hg_3d(const dgsem_ref_case& c) {
+  if constexpr (N == 3) {
+    if (c.volume_flux == 1) return make_hg_3d_vf<N, RanochaPlugin>(c);
+    if (c.volume_flux == 2) return make_hg_3d_vf<N, KennedyGruberPlugin>(c);
+  }
+  if (c.volume_flux != 0) return nullptr;
+  return make_hg_3d_vf<N, DGSEM::ChandrashekarFlux>(c);
+}
+
 template <std::size_t N>
 RefCaseBase* make_case_n(const dgsem_ref_case& c) {
   using Basis = DGSEM::Basis::LobattoLegendreBasis<T, N>;
@@ -449,13 +472,8 @@ RefCaseBase* make_case_n(const dgsem_ref_case& c) {
       using VF = DGSEM::VolumeIntegralSplitForm<Basis, E3, DGSEM::ChandrashekarFlux>;
       return new RefCase<E3, N, VF, decltype(b), 3>(c, E3{c.gamma}, b, true);
     }
-    case REF_EULER3D_PERIODIC_HG: {
-      using VF = DGSEM::VolumeIntegralShockCapturingHG<
-          Basis, E3, DGSEM::ChandrashekarFlux, DGSEM::LaxFriedrichsFlux,
-          DGSEM::HGIndicator<Basis, E3>>;
-      auto b = DGSEM::BoundarySet(P{}, P{}, P{}, P{}, P{}, P{});
-      return new RefCase<E3, N, VF, decltype(b), 3>(c, E3{c.gamma}, b, true);
-    }
+    case REF_EULER3D_PERIODIC_HG:
+      return make_hg_3d<N>(c);
     case REF_EULER2D_CENTRAL_DIRICHLET: {
       if constexpr (N == 3) {
         TravellingWave w;

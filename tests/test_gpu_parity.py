@@ -312,11 +312,11 @@ def test_launch_variants(name, cuda):
     torch.cuda.synchronize()
     for v in (1, 2):
         assert torch.equal(outs[0], outs[v]), v
-    # node-parallel shapes 3-4 (also with shock capturing) and the persistent
-    # shape 5 (no shock capturing): same arithmetic per flux, different
-    # summation order; 3, 4 and 5 give the same bits
-    node_variant = not case.get("viscous")
-    pipe_variant = node_variant and not case.get("shock_capturing")
+    # node-parallel shapes 3-4 (also with shock capturing or Navier-Stokes)
+    # and the persistent shape 5 (neither): same arithmetic per flux,
+    # different summation order; 3, 4 and 5 give the same bits
+    node_variant = True
+    pipe_variant = not case.get("shock_capturing") and not case.get("viscous")
     if node_variant:
         node_outs = []
         for v in ((3, 4, 5) if pipe_variant else (3, 4)):
