@@ -50,6 +50,7 @@ EXPORTED = [
     "dgsem_fp64_fma_peak", "dgsem_write_vtu", "dgsem_write_vtu_host",
     "dgsem_checkpoint_write", "dgsem_checkpoint_read", "dgsem_checkpoint_write_host",
     "dgsem_checkpoint_read_host", "dgsem_set_diagnostics", "dgsem_diagnostics",
+    "dgsem_geometry_from_coordinates",
 ]
 
 
@@ -149,6 +150,8 @@ def lib() -> ctypes.CDLL:
     L.dgsem_set_diagnostics.argtypes = [vp, c.c_int]
     L.dgsem_diagnostics.argtypes = [vp, c.POINTER(c.c_double), c.POINTER(c.c_double),
                                     c.POINTER(c.c_double)]
+    L.dgsem_geometry_from_coordinates.argtypes = [c.c_int, c.c_int, c.POINTER(c.c_int64), vp, vp,
+                                                   vp, vp]
     for name in EXPORTED:
         f = getattr(L, name)
         if name != "dgsem_status_string":

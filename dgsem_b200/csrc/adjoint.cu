@@ -78,10 +78,12 @@ class AdjointEngine final : public AdjointEngineBase {
       ga.gamma = cfg.gamma;
       ga.tab = cfg.tab;
       ga.basis = a.basis;
-      br1_gradient_kernel<N, EPB><<<blocks, EPB * N * N, 0, s>>>(ga);
-      adj_viscous_kernel<N, EPB><<<blocks, EPB * N * N, 0, s>>>(a);
+      // programmatic dependent launches: each kernel's blocks are placed while
+      // the previous one drains; griddepcontrol.wait orders the memory
+      launch_stage_kernel(br1_gradient_kernel<N, EPB>, blocks, EPB * N * N, 0, s, ga);
+      launch_stage_kernel(adj_viscous_kernel<N, EPB>, blocks, EPB * N * N, 0, s, a);
     }
-    adj_main_kernel<N, NS, EPB><<<blocks, EPB * N * N, 0, s>>>(a);
+    launch_stage_kernel(adj_main_kernel<N, NS, EPB>, blocks, EPB * N * N, 0, s, a);
     return cudaGetLastError();
   }
   int kernels_per_vjp() const override { return NS ? 3 : 1; }

@@ -203,6 +203,7 @@ template <int N, int EPB>
 __global__ void __launch_bounds__(EPB* N* N) adj_viscous_kernel(const AdjArgs<N> p) {
   constexpr int ND = N * N;
   __shared__ double ws[EPB][4][ND];
+  stage_dependency_sync();  // programmatic dependent launch (see launch_stage_kernel)
   const int tid = threadIdx.x;
   const int el = tid / ND, node = tid % ND;
   const int e = (int)blockIdx.x * EPB + el;
@@ -299,6 +300,7 @@ __global__ void __launch_bounds__(EPB* N* N) adj_main_kernel(const AdjArgs<N> p)
   __shared__ double ws[EPB][4][ND];
   __shared__ double ps[EPB][5][ND];  // rho, v1, v2, beta, kin
   __shared__ double xys[EPB][NXY][ND];
+  stage_dependency_sync();  // programmatic dependent launch (see launch_stage_kernel)
   const int tid = threadIdx.x;
   const int el = tid / ND, node = tid % ND;
   const int e = (int)blockIdx.x * EPB + el;

@@ -62,6 +62,7 @@ template <int N, int EPB>
 __global__ void __launch_bounds__(EPB* N* N) br1_gradient_kernel(const GradArgs<N> p) {
   constexpr int ND = N * N, NV = 4, NG = 4;
   __shared__ double qs[EPB][NG][ND];
+  stage_dependency_sync();  // programmatic dependent launch (see launch_stage_kernel)
   const int tid = threadIdx.x;
   const int el = tid / ND;
   const int node = tid % ND;

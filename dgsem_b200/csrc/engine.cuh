@@ -337,8 +337,8 @@ class Engine final : public EngineBase {
       ga.tab = cfg.tab;
       ga.basis = args.basis;
       const int64_t gblocks = (cfg.nelem + GRAD_EPB - 1) / GRAD_EPB;
-      br1_gradient_kernel<N, GRAD_EPB>
-          <<<(unsigned)gblocks, GRAD_EPB * N * N, 0, s>>>(ga);
+      launch_stage_kernel(br1_gradient_kernel<N, GRAD_EPB>, (unsigned)gblocks, GRAD_EPB * N * N, 0,
+                          s, ga);
     }
     switch (variant_) {
       case 1: launch<1>(args, cfg.nelem, s); break;

@@ -397,6 +397,23 @@ dgsem_status dgsem_checkpoint_write_host(const dgsem_mesh_desc* mesh,
 dgsem_status dgsem_checkpoint_read_host(const dgsem_mesh_desc* mesh, double* u_host,
                                         double* time, int64_t* step, const char* path);
 
+/* Per-node geometry of an arbitrary structured mesh (curvilinear included),
+ * computed on the device from its node coordinates with the reference's
+ * formulas and operation order, bit for bit: Jacobian matrix, contravariant
+ * vectors (2D adjugate, 3D conservative curl form) and inverse Jacobian
+ * (StructuredContainerInitializer::calc_jacobian_matrix /
+ * calc_contravariant_vectors / calc_inverse_jacobian,
+ * containers/data_container.hpp:230-312, 420-692; the reference runs them on
+ * the host inside StructuredElementInitializer::init_elements, :729-772).
+ * Device arrays, element e = ie + nx*(je + ny*ke), node = i + n*(j + n*k):
+ *   x[(e*d + c)*n^d + node]           node coordinates (input)
+ *   ja[((e*d + a)*d + c)*n^d + node]  contravariant vector Ja^a_c (output)
+ *   inv_j[e*n^d + node]               1/J (output)
+ * n <= 8 in 2D, n <= 5 in 3D.  Asynchronous on `stream` (a cudaStream_t). */
+dgsem_status dgsem_geometry_from_coordinates(int ndims, int polydeg,
+                                             const int64_t* n_cells, const double* x,
+                                             double* ja, double* inv_j, void* stream);
+
 /* Host-side copies of the basis tables (nodes, weights, inv_weights,
  * lhat(-1), lhat(+1), D, Dsplit, Dhat, inverse Legendre Vandermonde; the
  * n x n tables row-major) for polydeg N; out needs 5n + 4n^2 doubles.

@@ -235,6 +235,11 @@ __device__ inline std::array<T, NV> reflect(const std::array<T, NV>& ui,
 
 // ---- kernel arguments --------------------------------------------------------
 template <int N>
+struct PluginNodes {
+  double xi[N];  // Lobatto-Legendre nodes on [-1, 1]
+};
+
+template <int N>
 struct PluginBasis {
   double Dsplit[N][N];
   double lhat_l0;  // l_0(-1) / w_0
@@ -433,6 +438,35 @@ __global__ void __launch_bounds__(EPB* ipow(N, (int)Eq::NDIMS))
   }
 }
 
+// Node coordinates of a structured mesh as the image of the reference square
+// or cube [-1, 1]^d under a mapping (StructuredContainerInitializer::
+// calc_node_coordinates, containers/data_container.hpp:196-225): element ie
+// covers [-1 + ie dx, -1 + (ie + 1) dx] with dx = 2 / n_cells, node i sits at
+// its centre + (dx / 2) xi_i, and x = mapping.eval(reference point).  Mapping
+// is any device-callable type with std::array<double, DIM> eval(const
+// std::array<double, DIM>&) const (the reference's LinearMapping interface,
+// base/mapping.hpp:31-50).  One thread per node; x[(e*DIM + c)*ND + node].
+template <class Mapping, int DIM, int N>
+__global__ void map_nodes_kernel(Mapping map, int c0, int c1, int c2, PluginNodes<N> gll,
+                                 double* x) {
+  constexpr int ND = ipow(N, DIM);
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nelem = (long long)c0 * c1 * (DIM == 3 ? c2 : 1);
+  if (idx >= nelem * ND) return;
+  const int e = (int)(idx / ND), node = (int)(idx % ND);
+  const int ev[3] = {e % c0, (e / c0) % c1, DIM == 3 ? e / (c0 * c1) : 0};
+  const int iv[3] = {node % N, (node / N) % N, node / (N * N)};
+  const int cells[3] = {c0, c1, c2};
+  std::array<double, DIM> ref;
+  for (int a = 0; a < DIM; ++a) {
+    const double dx = __ddiv_rn(2.0, (double)cells[a]);
+    const double off = __dadd_rn(__dadd_rn(-1.0, __dmul_rn((double)ev[a], dx)), __dmul_rn(0.5, dx));
+    ref[a] = __dadd_rn(off, __dmul_rn(__dmul_rn(0.5, dx), gll.xi[iv[a]]));
+  }
+  const std::array<double, DIM> p = map.eval(ref);
+  for (int a = 0; a < DIM; ++a) x[((long long)e * DIM + a) * ND + node] = p[a];
+}
+
 // ---- host side -----------------------------------------------------------------
 namespace detail {
 inline void check(dgsem_status s, const char* where) {
@@ -511,6 +545,35 @@ class StructuredSolver {
     detail::check_cuda(cudaMemcpy(x_, x_dev, E * DIM * ND * sizeof(double),
                                   cudaMemcpyDeviceToDevice), "cudaMemcpy");
   }
+
+  // Any mapping of the reference square / cube (map_nodes_kernel): node
+  // coordinates and per-node metrics are computed on the device
+  // (dgsem_geometry_from_coordinates, the reference's metric formulas).
+  template <class Mapping>
+  StructuredSolver(const Eq& eq, const Mapping& map, const std::array<int, DIM>& cells,
+                   const Bcs& bcs, cudaStream_t stream = nullptr)
+      : eq_(eq), bcs_(bcs), stream_(stream) {
+    set_mesh(cells);
+    alloc_geometry();
+    std::vector<double> tab(5 * N + 4 * N * N);
+    detail::check(dgsem_basis_tables_host((int)Polydeg, tab.data()), "dgsem_basis_tables_host");
+    PluginNodes<N> gll;
+    for (int i = 0; i < N; ++i) gll.xi[i] = tab[i];
+    const long long total = (long long)nelem_ * ND;
+    map_nodes_kernel<Mapping, DIM, N><<<(unsigned)((total + 127) / 128), 128, 0, stream_>>>(
+        map, cells_[0], cells_[1], cells_[2], gll, x_);
+    detail::check_cuda(cudaGetLastError(), "map_nodes_kernel");
+    const int64_t c64[3] = {cells_[0], cells_[1], cells_[2]};
+    detail::check(dgsem_geometry_from_coordinates(DIM, (int)Polydeg, c64, x_, ja_, inv_j_,
+                                                  stream_),
+                  "dgsem_geometry_from_coordinates");
+    detail::check_cuda(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+  }
+
+  // device geometry (ja, inv_j, x) in the layout of PluginGeometry
+  const double* geometry_ja() const { return ja_; }
+  const double* geometry_inv_j() const { return inv_j_; }
+  const double* geometry_x() const { return x_; }
 
   StructuredSolver(const StructuredSolver&) = delete;
   StructuredSolver& operator=(const StructuredSolver&) = delete;

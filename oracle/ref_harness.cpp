@@ -44,6 +44,8 @@ enum {
   REF_EULER3D_PERIODIC_HG = 4,     // 3D periodic + HG
   REF_NS2D_PERIODIC_SPLIT = 5,     // Navier-Stokes BR1 + split form
   REF_EULER2D_CENTRAL_DIRICHLET = 6,  // the reference's CentralFlux + user DirichletBC
+  REF_EULER2D_CURVED_CENTRAL = 7,     // curvilinear periodic mesh, CentralFlux + LLF
+  REF_EULER3D_CURVED = 8,             // curvilinear periodic mesh, Chandrashekar + LLF
 };
 
 typedef struct {
@@ -102,6 +104,27 @@ struct TravellingWave {
     const T u = T(0.3), v = T(-0.2);
     const T p = T(1) + T(0.1) * std::cos(pi * (x[0] - x[1]));
     return {rho, rho * u, rho * v, p / T(0.4) + T(0.5) * rho * (u * u + v * v)};
+  }
+};
+
+// A curvilinear mapping of the reference square / cube [-1, 1]^D with the
+// reference's Mapping interface (eval, base/mapping.hpp:31-50): the linear
+// map onto [left, right] plus a displacement that vanishes on the boundary,
+// so the mesh stays periodic.  The same formula is the device mapping of the
+// curvilinear tests (tests/cpp/plugin_curved.cu).
+template <std::size_t D>
+struct CurvedMapping {
+  std::array<T, D> left{}, right{};
+  T amp = T(0.05);
+  std::array<T, D> eval(const std::array<T, D>& xi) const {
+    const T pi = static_cast<T>(3.14159265358979323846);
+    const std::array<T, D> lin = DGSEM::linear_interpolate(xi, left, right);
+    T bump = T(1);
+    for (std::size_t a = 0; a < D; ++a) bump *= std::sin(pi * xi[a]);
+    std::array<T, D> x{};
+    for (std::size_t a = 0; a < D; ++a)
+      x[a] = lin[a] + amp * (right[a] - left[a]) * bump * (a == 0 ? T(1) : T(-0.5));
+    return x;
   }
 };
 
@@ -425,6 +448,64 @@ RefCaseBase* make_hg_3d(const dgsem_ref_case& c) {
   return make_hg_3d_vf<N, DGSEM::ChandrashekarFlux>(c);
 }
 
+// RefCase on a mesh given by an arbitrary Mapping: the reference's
+// StructuredElementInitializer with that mapping fills the element container,
+// which the solver's 4-argument constructor takes as is
+// (solver/structured_solver.hpp:36-42).
+template <class Eq, std::size_t N, class VolumeFlux, class Boundaries, std::size_t D,
+          class Mapping, class SurfaceFlux = DGSEM::LaxFriedrichsFlux<Eq>>
+class MappedRefCase final : public RefCaseBase {
+ public:
+  using Basis = DGSEM::Basis::LobattoLegendreBasis<T, N>;
+  using Mesh = DGSEM::StructuredMesh<T, D>;
+  using Container = DGSEM::StructuredElementContainer<T, D>;
+  using Solver = DGSEM::StructuredSolver<Eq, Basis, VolumeFlux, SurfaceFlux, Mesh, Boundaries>;
+  using Sol = DGSEM::Solution<Mesh, Basis, Eq>;
+
+  MappedRefCase(const dgsem_ref_case& c, const Eq& eq, const Boundaries& bcs, const Mapping& map)
+      : mesh_(RefCase<Eq, N, VolumeFlux, Boundaries, D>::make_left(c),
+              RefCase<Eq, N, VolumeFlux, Boundaries, D>::make_right(c),
+              RefCase<Eq, N, VolumeFlux, Boundaries, D>::make_cells(c)),
+        container_(init_container(c, map)),
+        solver_(eq, mesh_, container_, bcs),
+        sol_(mesh_) {}
+
+  static Container init_container(const dgsem_ref_case& c, const Mapping& map) {
+    Container k;
+    std::array<bool, D> per{};
+    per.fill(true);
+    DGSEM::StructuredElementInitializer<T, Basis, Mapping, D> init(map, per);
+    init.init_elements(RefCase<Eq, N, VolumeFlux, Boundaries, D>::make_cells(c), k);
+    return k;
+  }
+
+  std::size_t state_size() const override { return sol_.u_device.size(); }
+  void rhs(const T* u, T* du, T t) override {
+    std::memcpy(sol_.u_device.data(), u, state_size() * sizeof(T));
+    solver_.calc_rhs(sol_, t);
+    std::memcpy(du, sol_.du_device.data(), state_size() * sizeof(T));
+  }
+  void alpha(const T*, T*) override {}
+  void steps(T*, T, T, int) override {}
+  void geometry(T* coords, T* ja, T* inv_j) override {
+    if (coords)
+      std::memcpy(coords, container_.node_coordinates.data(),
+                  container_.node_coordinates.size() * sizeof(T));
+    if (ja)
+      std::memcpy(ja, container_.contravariant_vectors.data(),
+                  container_.contravariant_vectors.size() * sizeof(T));
+    if (inv_j)
+      std::memcpy(inv_j, container_.inverse_jacobian.data(),
+                  container_.inverse_jacobian.size() * sizeof(T));
+  }
+
+ private:
+  Mesh mesh_;
+  Container container_;
+  Solver solver_;
+  Sol sol_;
+};
+
 template <std::size_t N>
 RefCaseBase* make_case_n(const dgsem_ref_case& c) {
   using Basis = DGSEM::Basis::LobattoLegendreBasis<T, N>;
@@ -484,6 +565,34 @@ RefCaseBase* make_case_n(const dgsem_ref_case& c) {
       }
       return nullptr;
     }
+    case REF_EULER2D_CURVED_CENTRAL: {
+      if constexpr (N == 3) {
+        CurvedMapping<2> map;
+        for (int a = 0; a < 2; ++a) {
+          map.left[a] = c.left[a];
+          map.right[a] = c.right[a];
+        }
+        auto b = DGSEM::BoundarySet(P{}, P{}, P{}, P{});
+        using VF = DGSEM::VolumeIntegralSplitForm<Basis, E2, DGSEM::CentralFlux>;
+        return new MappedRefCase<E2, N, VF, decltype(b), 2, CurvedMapping<2>>(c, E2{c.gamma}, b,
+                                                                              map);
+      }
+      return nullptr;
+    }
+    case REF_EULER3D_CURVED: {
+      if constexpr (N <= 4) {
+        CurvedMapping<3> map;
+        for (int a = 0; a < 3; ++a) {
+          map.left[a] = c.left[a];
+          map.right[a] = c.right[a];
+        }
+        auto b = DGSEM::BoundarySet(P{}, P{}, P{}, P{}, P{}, P{});
+        using VF = DGSEM::VolumeIntegralSplitForm<Basis, E3, DGSEM::ChandrashekarFlux>;
+        return new MappedRefCase<E3, N, VF, decltype(b), 3, CurvedMapping<3>>(c, E3{c.gamma}, b,
+                                                                              map);
+      }
+      return nullptr;
+    }
     case REF_NS2D_PERIODIC_SPLIT: {
       using VF = DGSEM::VolumeIntegralSplitForm<Basis, NS2, DGSEM::ChandrashekarFlux>;
       auto b = DGSEM::BoundarySet(P{}, P{}, P{}, P{});
@@ -497,7 +606,7 @@ RefCaseBase* make_case_n(const dgsem_ref_case& c) {
 
 RefCaseBase* make_case(const dgsem_ref_case& c) {
   const bool is3d = c.kind == REF_EULER3D_PERIODIC_SPLIT ||
-                    c.kind == REF_EULER3D_PERIODIC_HG;
+                    c.kind == REF_EULER3D_PERIODIC_HG || c.kind == REF_EULER3D_CURVED;
   if (is3d) {
     switch (c.polydeg) {
       case 1: return make_case_n<1>(c);
