@@ -10,7 +10,8 @@ from .solver import (  # noqa: F401
     CompressibleNavierStokes2D, DirichletBC, DoubleMachReflectionInitial, HGIndicator,
     HLLCFlux, InviscidTaylorGreenVortex, IsentropicVortex, KelvinHelmholtzInitial,
     KennedyGruberFlux, LaxFriedrichsFlux, LobattoLegendreBasis,
-    MixedDirichletSlipWallBC, OutflowBC, PeriodicBC, RanochaFlux, SlipWallBC, Solution,
+    MixedDirichletSlipWallBC, NSNoSlipAdiabaticWallBC, NSSlipAdiabaticWallBC, OutflowBC,
+    PeriodicBC, RanochaFlux, SlipWallBC, Solution,
     SSPRK3, StructuredMesh, StructuredSolver, TaylorGreenVortex2D,
     VolumeIntegralShockCapturingHG, VolumeIntegralSplitForm,
 )

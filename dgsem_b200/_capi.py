@@ -29,6 +29,7 @@ SF_LAX_FRIEDRICHS, SF_HLLC = 0, 1
 VI_SPLIT_FORM, VI_SHOCK_CAPTURING_HG = 0, 1
 BC_PERIODIC, BC_DIRICHLET_DMR, BC_OUTFLOW, BC_MIXED_DMR_WALL = 0, 1, 2, 3
 BC_DIRICHLET_CONST, BC_SLIP_WALL = 4, 5
+BC_NS_NOSLIP_ADIABATIC_WALL, BC_NS_SLIP_ADIABATIC_WALL = 6, 7
 IC_KELVIN_HELMHOLTZ, IC_DOUBLE_MACH, IC_TAYLOR_GREEN_3D = 0, 1, 2
 IC_TAYLOR_GREEN_2D, IC_ISENTROPIC_VORTEX = 3, 4
 
@@ -50,7 +51,7 @@ EXPORTED = [
     "dgsem_fp64_fma_peak", "dgsem_write_vtu", "dgsem_write_vtu_host",
     "dgsem_checkpoint_write", "dgsem_checkpoint_read", "dgsem_checkpoint_write_host",
     "dgsem_checkpoint_read_host", "dgsem_set_diagnostics", "dgsem_diagnostics",
-    "dgsem_geometry_from_coordinates",
+    "dgsem_geometry_from_coordinates", "dgsem_batch_set_persistent",
 ]
 
 
@@ -152,6 +153,7 @@ def lib() -> ctypes.CDLL:
                                     c.POINTER(c.c_double)]
     L.dgsem_geometry_from_coordinates.argtypes = [c.c_int, c.c_int, c.POINTER(c.c_int64), vp, vp,
                                                    vp, vp]
+    L.dgsem_batch_set_persistent.argtypes = [vp, c.c_int]
     for name in EXPORTED:
         f = getattr(L, name)
         if name != "dgsem_status_string":

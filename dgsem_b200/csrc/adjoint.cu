@@ -78,6 +78,8 @@ class AdjointEngine final : public AdjointEngineBase {
       ga.gamma = cfg.gamma;
       ga.tab = cfg.tab;
       ga.basis = a.basis;
+      ga.periodic[0] = ga.periodic[1] = 1;  // the adjoint covers periodic meshes
+      for (int f = 0; f < 4; ++f) ga.bc_kind[f] = 0;
       // programmatic dependent launches: each kernel's blocks are placed while
       // the previous one drains; griddepcontrol.wait orders the memory
       launch_stage_kernel(br1_gradient_kernel<N, EPB>, blocks, EPB * N * N, 0, s, ga);

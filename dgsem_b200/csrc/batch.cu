@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/dgsem_b200.h"
+#include "batch_persistent.hpp"
 #include "engine.cuh"
 #include "tables.hpp"
 
@@ -61,6 +62,15 @@ struct dgsem_batch {
   const double* views_u = nullptr;  // key of the uploaded views
   std::vector<double> views_dt;
   int64_t launches = 0;
+  // persistent mode: one launch per stage over all meshes (2D, LLF)
+  bool persistent = false;
+  bool persistent_ok = false;
+  int* work = nullptr;  // device work list: (n << 24) | tile
+  int nwork = 0;
+  int* ptile_mesh[7] = {};  // per degree n = k + 2: tile lists of the persistent launch
+  int* ptile_e0[7] = {};
+  size_t psmem = 0;
+  int pgrid = 0;
 };
 
 struct dgsem_batch_graph {
@@ -68,6 +78,7 @@ struct dgsem_batch_graph {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int nsteps = 0;
+  bool persistent = false;  // captured in persistent mode
 };
 
 namespace {
@@ -138,6 +149,21 @@ dgsem_status launch_stage(dgsem_batch* b, int stage, double t, const double* t_d
   static const double TOFF[3] = {0.0, 1.0, 0.5};  // fractions of dt (periodic: unused)
   (void)TOFF;
   const MeshView* views = b->views + (size_t)(stage - 1) * b->nmeshes;
+  if (b->persistent) {
+    PersistentDegree deg[7];
+    for (const Group& g : b->groups) {
+      PersistentDegree& d = deg[g.n - 2];
+      d.cfg = &g.cfg;
+      d.meshes = views;
+      d.tile_mesh = b->ptile_mesh[g.n - 2];
+      d.tile_e0 = b->ptile_e0[g.n - 2];
+    }
+    cudaError_t e = launch_persistent_stage(b->scheme.volume_flux, deg, b->work, b->nwork,
+                                            A[stage - 1], B[stage - 1], t, t_dev, b->pgrid,
+                                            b->psmem, main);
+    b->launches++;
+    return st_of(e);
+  }
   if (cudaEventRecord(b->fork, main) != cudaSuccess) return DGSEM_ERR_CUDA;
   for (Group& g : b->groups) {
     if (cudaStreamWaitEvent(g.stream, b->fork, 0) != cudaSuccess) return DGSEM_ERR_CUDA;
@@ -149,6 +175,48 @@ dgsem_status launch_stage(dgsem_batch* b, int stage, double t, const double* t_d
     b->launches++;
   }
   return DGSEM_OK;
+}
+
+// Work list of the persistent launch: every tile of every degree, higher
+// degrees (costlier tiles) first, so that the blocks' round-robin walk ends
+// with the cheap tiles.
+cudaError_t build_persistent(dgsem_batch* b) {
+  b->persistent_ok = persistent_supported(b->ndims, b->scheme.volume_flux,
+                                          b->scheme.surface_flux);
+  if (!b->persistent_ok) return cudaSuccess;
+  std::vector<int> work;
+  PersistentDegree deg[7];
+  std::vector<Group*> order;
+  for (Group& g : b->groups) order.push_back(&g);
+  std::sort(order.begin(), order.end(), [](Group* x, Group* y) { return x->n > y->n; });
+  for (Group* g : order) {
+    const int k = g->n - 2;
+    const int epb = persistent_elements_per_tile(g->n);
+    std::vector<int> tm, te;
+    for (int m : g->members)
+      for (int64_t e0 = 0; e0 < b->nelem[m]; e0 += epb) {
+        work.push_back((g->n << 24) | (int)tm.size());
+        tm.push_back(m);
+        te.push_back((int)e0);
+      }
+    b->ptile_mesh[k] = balloc<int>(b, tm.size());
+    b->ptile_e0[k] = balloc<int>(b, te.size());
+    if (!b->ptile_mesh[k] || !b->ptile_e0[k]) return cudaErrorMemoryAllocation;
+    cudaError_t e = cudaMemcpy(b->ptile_mesh[k], tm.data(), tm.size() * sizeof(int),
+                               cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(b->ptile_e0[k], te.data(), te.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return e;
+    deg[k].cfg = &g->cfg;
+  }
+  b->nwork = (int)work.size();
+  b->work = balloc<int>(b, work.size());
+  if (!b->work) return cudaErrorMemoryAllocation;
+  cudaError_t e = cudaMemcpy(b->work, work.data(), work.size() * sizeof(int),
+                             cudaMemcpyHostToDevice);
+  b->psmem = persistent_smem(b->scheme.volume_flux, deg);
+  b->pgrid = persistent_grid(b->scheme.volume_flux, b->psmem);
+  return e;
 }
 
 cudaError_t build_tiles(const dgsem_batch* b, Group& g) {
@@ -363,6 +431,7 @@ dgsem_status dgsem_batch_create(const dgsem_mesh_desc* meshes, int n_meshes,
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming);
     b->groups.push_back(std::move(g));
   }
+  if (e == cudaSuccess) e = build_persistent(b);
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     bfree(b);
@@ -426,6 +495,7 @@ dgsem_status dgsem_batch_graph_create(dgsem_batch* b, double* u, const double* d
   }
   g->batch = b;
   g->nsteps = nsteps;
+  g->persistent = b->persistent;
   cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     for (int s = 0; s < nsteps && st == DGSEM_OK; ++s)
@@ -451,7 +521,8 @@ dgsem_status dgsem_batch_graph_create(dgsem_batch* b, double* u, const double* d
 
 dgsem_status dgsem_batch_graph_launch(dgsem_batch_graph* g) {
   if (!g || !g->exec) return DGSEM_ERR_INVALID_ARG;
-  g->batch->launches += 3 * (int64_t)g->nsteps * g->batch->groups.size();
+  g->batch->launches +=
+      3 * (int64_t)g->nsteps * (g->persistent ? 1 : (int64_t)g->batch->groups.size());
   return st_of(cudaGraphLaunch(g->exec, g->batch->stream));
 }
 
@@ -474,6 +545,13 @@ dgsem_status dgsem_batch_check_finite(dgsem_batch* b) {
     cudaStreamSynchronize(b->stream);
     return DGSEM_ERR_NONFINITE;
   }
+  return DGSEM_OK;
+}
+
+dgsem_status dgsem_batch_set_persistent(dgsem_batch* b, int enable) {
+  if (!b) return DGSEM_ERR_INVALID_ARG;
+  if (enable && !b->persistent_ok) return DGSEM_ERR_UNSUPPORTED;
+  b->persistent = enable != 0;
   return DGSEM_OK;
 }
 

@@ -56,6 +56,8 @@ struct GradArgs {
   double gamma;
   DeviceTables tab;
   BasisConst<N> basis;
+  int periodic[2];  // per direction; otherwise the faces carry wall BCs
+  int bc_kind[4];   // BcKind per face (left, right, bottom, top)
 };
 
 template <int N, int EPB>
@@ -109,6 +111,30 @@ __global__ void __launch_bounds__(EPB* N* N) br1_gradient_kernel(const GradArgs<
       if ((side == 0 && pos != 0) || (side == 1 && pos != N - 1)) continue;
       ElemIdx<2> nb = ei;
       const int64_t nc = p.cells[dir];
+      const int64_t npos = ei.i[dir] + (side ? 1 : -1);
+      const double factor = side ? p.basis.lhat_rN : -p.basis.lhat_l0;
+      if (!p.periodic[dir] && (npos < 0 || npos >= nc)) {
+        // wall: q^ = q of the wall state (navier_stokes_wall_boundary.hpp:
+        // 82-99 no-slip: velocity zero; :162-190 slip: the normal velocity
+        // removed along the element's own face normal)
+        double qw[NG];
+#pragma unroll
+        for (int v = 0; v < NG; ++v) qw[v] = q[v];
+        if (p.bc_kind[2 * dir + side] == BC_NS_NOSLIP_ADIABATIC_WALL) {
+          qw[1] = 0.0;
+          qw[2] = 0.0;
+        } else {
+          const double n0 = ja[dir][0], n1 = ja[dir][1];
+          const double vn = (qw[1] * n0 + qw[2] * n1) / (n0 * n0 + n1 * n1);
+          qw[1] -= vn * n0;
+          qw[2] -= vn * n1;
+        }
+#pragma unroll
+        for (int v = 0; v < NG; ++v)
+#pragma unroll
+          for (int d = 0; d < 2; ++d) g[v][d] += factor * qw[v] * ja[dir][d];
+        continue;
+      }
       nb.i[dir] = (ei.i[dir] + (side ? 1 : nc - 1)) % nc;
       const int64_t en = elem_linear<2>(nb, p.cells);
       const int nb_node = dir == 0 ? ((side ? 0 : N - 1) + N * j) : (i + N * (side ? 0 : N - 1));
@@ -116,7 +142,6 @@ __global__ void __launch_bounds__(EPB* N* N) br1_gradient_kernel(const GradArgs<
 #pragma unroll
       for (int v = 0; v < NV; ++v) un[v] = __ldg(p.u + (en * NV + v) * ND + nb_node);
       ns_gradient_variables(un, p.gamma, qn);
-      const double factor = side ? p.basis.lhat_rN : -p.basis.lhat_l0;
 #pragma unroll
       for (int v = 0; v < NG; ++v) {
         // q^ = 0.5 (q_left + q_right): the left state is the low-side element's

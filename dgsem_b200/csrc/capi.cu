@@ -178,7 +178,10 @@ dgsem_status validate(const dgsem_mesh_desc* m, const dgsem_scheme_desc* s) {
   if (s->volume_integral < 0 || s->volume_integral > 1) return DGSEM_ERR_INVALID_ARG;
   if (!(s->gamma > 1.0)) return DGSEM_ERR_INVALID_ARG;
   for (int f = 0; f < 2 * m->ndims; ++f) {
-    if (s->bc[f] < 0 || s->bc[f] > 5) return DGSEM_ERR_INVALID_ARG;
+    if (s->bc[f] < 0 || s->bc[f] > 7) return DGSEM_ERR_INVALID_ARG;
+    const bool ns_wall = s->bc[f] == DGSEM_BC_NS_NOSLIP_ADIABATIC_WALL ||
+                         s->bc[f] == DGSEM_BC_NS_SLIP_ADIABATIC_WALL;
+    if (ns_wall && s->equation != DGSEM_NAVIER_STOKES_2D) return DGSEM_ERR_UNSUPPORTED;
     if (m->ndims == 3 && s->bc[f] != DGSEM_BC_PERIODIC) return DGSEM_ERR_UNSUPPORTED;
   }
   for (int d = 0; d < m->ndims; ++d) {
@@ -193,8 +196,11 @@ dgsem_status validate(const dgsem_mesh_desc* m, const dgsem_scheme_desc* s) {
   }
   if (s->equation == DGSEM_NAVIER_STOKES_2D) {
     if (s->volume_integral != DGSEM_VI_SPLIT_FORM) return DGSEM_ERR_UNSUPPORTED;
+    // periodic directions or the Navier-Stokes adiabatic walls
     for (int f = 0; f < 4; ++f)
-      if (s->bc[f] != DGSEM_BC_PERIODIC) return DGSEM_ERR_UNSUPPORTED;
+      if (s->bc[f] != DGSEM_BC_PERIODIC && s->bc[f] != DGSEM_BC_NS_NOSLIP_ADIABATIC_WALL &&
+          s->bc[f] != DGSEM_BC_NS_SLIP_ADIABATIC_WALL)
+        return DGSEM_ERR_UNSUPPORTED;
     if (!(s->mu >= 0.0) || !(s->prandtl > 0.0)) return DGSEM_ERR_INVALID_ARG;
   }
   return DGSEM_OK;

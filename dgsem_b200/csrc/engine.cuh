@@ -100,6 +100,34 @@ inline void fill_basis_const(const BasisTables& b, BasisConst<N>* out) {
   out->lhat_rN = b.lhat_right[N - 1];
 }
 
+// The arguments of one stage launch that do not depend on the mesh.
+template <int N>
+inline StageArgs<N> stage_args_common(const EngineConfig& cfg, double a, double b, double t,
+                                      const double* t_dev, double* alpha_out) {
+  StageArgs<N> args{};
+  args.a = a;
+  args.b = b;
+  args.t = t;
+  args.t_dev = t_dev;
+  args.gamma = cfg.gamma;
+  args.inv_gm1 = 1.0 / (cfg.gamma - 1.0);
+  args.alpha_max = cfg.alpha_max;
+  args.alpha_min = cfg.alpha_min;
+  args.atol = cfg.atol;
+  args.hg_threshold = cfg.hg_threshold;
+  args.hg_s = cfg.hg_s;
+  args.alpha_out = alpha_out;
+  args.nonfinite = cfg.nonfinite;
+  args.grad = cfg.grad;
+  args.mu = cfg.mu;
+  args.kappa = cfg.gamma / ((cfg.gamma - 1.0) * cfg.prandtl);
+  args.bc = cfg.bc;
+  args.wait_limit_ns = cfg.wait_limit_ns;
+  args.skip_tile_copy = cfg.skip_tile_copy;
+  fill_basis_const<N>(cfg.basis, &args.basis);
+  return args;
+}
+
 // Launch geometry per (DIM, N, variant): one thread per element line.
 //   variant 0: ~128 (2D) / ~96 (3D) threads per block, no register cap
 //   variant 1: same block, register cap for one more resident block per SM
@@ -275,28 +303,7 @@ class Engine final : public EngineBase {
 
   StageArgs<N> common_args(const EngineConfig& cfg, double a, double b, double t,
                            const double* t_dev, double* alpha_out) const {
-    StageArgs<N> args{};
-    args.a = a;
-    args.b = b;
-    args.t = t;
-    args.t_dev = t_dev;
-    args.gamma = cfg.gamma;
-    args.inv_gm1 = 1.0 / (cfg.gamma - 1.0);
-    args.alpha_max = cfg.alpha_max;
-    args.alpha_min = cfg.alpha_min;
-    args.atol = cfg.atol;
-    args.hg_threshold = cfg.hg_threshold;
-    args.hg_s = cfg.hg_s;
-    args.alpha_out = alpha_out;
-    args.nonfinite = cfg.nonfinite;
-    args.grad = cfg.grad;
-    args.mu = cfg.mu;
-    args.kappa = cfg.gamma / ((cfg.gamma - 1.0) * cfg.prandtl);
-    args.bc = cfg.bc;
-    args.wait_limit_ns = cfg.wait_limit_ns;
-    args.skip_tile_copy = cfg.skip_tile_copy;
-    fill_basis_const<N>(cfg.basis, &args.basis);
-    return args;
+    return stage_args_common<N>(cfg, a, b, t, t_dev, alpha_out);
   }
 
   template <int V>
@@ -336,6 +343,8 @@ class Engine final : public EngineBase {
       ga.gamma = cfg.gamma;
       ga.tab = cfg.tab;
       ga.basis = args.basis;
+      for (int d = 0; d < 2; ++d) ga.periodic[d] = cfg.periodic[d];
+      for (int f = 0; f < 4; ++f) ga.bc_kind[f] = cfg.bc.kind[f];
       const int64_t gblocks = (cfg.nelem + GRAD_EPB - 1) / GRAD_EPB;
       launch_stage_kernel(br1_gradient_kernel<N, GRAD_EPB>, (unsigned)gblocks, GRAD_EPB * N * N, 0,
                           s, ga);

@@ -58,7 +58,9 @@ enum BcKind : int {
   BC_OUTFLOW = 2,
   BC_MIXED_DMR_WALL = 3,
   BC_DIRICHLET_CONST = 4,
-  BC_SLIP_WALL = 5
+  BC_SLIP_WALL = 5,
+  BC_NS_NOSLIP_ADIABATIC_WALL = 6,  // navier_stokes_wall_boundary.hpp:33-132
+  BC_NS_SLIP_ADIABATIC_WALL = 7     // navier_stokes_wall_boundary.hpp:134-219
 };
 
 struct BcParams {
@@ -658,6 +660,13 @@ __device__ __forceinline__ void element_face_flux_state(
       }
 #pragma unroll
       for (int v = 0; v < 4; ++v) f[v] += w[0][v] * nrm[0] + w[1][v] * nrm[1];
+    } else if (p.bc.kind[face] == BC_NS_NOSLIP_ADIABATIC_WALL) {
+      // NSNoSlipAdiabaticWallBC::apply_viscous_device (navier_stokes_wall_
+      // boundary.hpp:101-131): the inner -F_v . n on the momentum, no mass
+      // or energy flux (adiabatic); the slip wall adds nothing
+#pragma unroll
+      for (int v = 1; v < 3; ++v)
+        f[v] += wv_el[(0 * NV + v) * NDP + opn] * nrm[0] + wv_el[(1 * NV + v) * NDP + opn] * nrm[1];
     }
   }
 }

@@ -207,7 +207,7 @@ __device__ __forceinline__ void node_volume_direction(const StageArgs<N>& p, con
                                                       const NodeFluxState<DIM>& own,
                                                       double hgm1, double* acc,
                                                       double* xbuf = nullptr, int tid = 0,
-                                                      int nth = 0) {
+                                                      int nth = 0, bool in_range = true) {
   constexpr int NV = DIM + 2, ND = ipow(N, DIM);
   constexpr bool HALF = NodeKernelSlots<DIM, VF>::HALF;
   // node-index and shared-memory-index strides along DIR
@@ -264,20 +264,22 @@ __device__ __forceinline__ void node_volume_direction(const StageArgs<N>& p, con
       for (int q = 0; q < NV; ++q)
         acc[q] += dmb * __shfl_sync(0xffffffffu, f[q], lane + back * SN);
     }
-    if (XCHG && o < N - o) {
+    if (XCHG && o < N - o && in_range) {
 #pragma unroll
       for (int q = 0; q < NV; ++q) xbuf[((o - 1) * NV + q) * nth + tid] = f[q];
     }
   }
   if constexpr (XCHG) {
     __syncthreads();
+    if (in_range) {
 #pragma unroll
-    for (int o = 1; o <= XR; ++o) {
-      const int back = m - o < 0 ? N - o : -o;
-      const double dmb = Dm[m + back];
+      for (int o = 1; o <= XR; ++o) {
+        const int back = m - o < 0 ? N - o : -o;
+        const double dmb = Dm[m + back];
 #pragma unroll
-      for (int q = 0; q < NV; ++q)
-        acc[q] += dmb * xbuf[((o - 1) * NV + q) * nth + tid + back * SN];
+        for (int q = 0; q < NV; ++q)
+          acc[q] += dmb * xbuf[((o - 1) * NV + q) * nth + tid + back * SN];
+      }
     }
     __syncthreads();  // the buffer is reused by the next direction
   }
@@ -337,8 +339,12 @@ __device__ __forceinline__ void node_fv_direction(const StageArgs<N>& p, const M
   }
 }
 
-template <int DIM, int N, int VF, int SF, int EPB, bool BATCH, bool HG, bool NS = false>
-__device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
+// NTB: threads of the launch (>= EPB * n^d; the threads past EPB * n^d only
+// take part in the block's barriers).  PERSIST: batched launches whose
+// tiles come from a work list (`tile`), without the bulk copy of u_n.
+template <int DIM, int N, int VF, int SF, int EPB, bool BATCH, bool HG, bool NS = false,
+          int NTB = 0, bool PERSIST = false>
+__device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile = 0) {
   static_assert(!NS || (DIM == 2 && !HG && !BATCH), "Navier-Stokes: 2D split form");
   using S = NodeShape<DIM, N, VF, EPB, HG, NS>;
   using K = NodeKernelSlots<DIM, VF>;
@@ -360,9 +366,12 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   const int tid = threadIdx.x;
   __shared__ MeshView mesh_s;
   int e0;
+  // threads past the element tile (wider persistent blocks) only join barriers
+  const bool worker = NTB == 0 || tid < NT;
   if constexpr (BATCH) {
-    e0 = p.tile_e0[blockIdx.x];
-    if (tid == 0) mesh_s = p.meshes[p.tile_mesh[blockIdx.x]];
+    const int tl = PERSIST ? tile : (int)blockIdx.x;
+    e0 = p.tile_e0[tl];
+    if (tid == 0) mesh_s = p.meshes[p.tile_mesh[tl]];
     __syncthreads();
   } else {
     e0 = (int)blockIdx.x * EPB;
@@ -379,7 +388,7 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   // arrives while the block computes (block-uniform decision).
   __shared__ uint64_t bar_n;
   bool bulk_n = false;
-  if constexpr (S::SM_N > 0)
+  if constexpr (S::SM_N > 0 && !PERSIST)
     bulk_n = p.a != 0.0 && (reinterpret_cast<uintptr_t>(M.u_n) & 15u) == 0;
   if (bulk_n && tid == 0) {
     const uint32_t bytes = (uint32_t)ne * NV * ND * sizeof(double);
@@ -430,7 +439,8 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   if constexpr (HG) {
     for (int k = tid; k < N * N; k += NT) vinv_s[k] = p.basis.Vinv[k / N][k % N];
   }
-  load_element_tile<N, NV, ND, NDP, EPB, NT>(M.u_in + (int64_t)e0 * NV * ND, us, ne, tid);
+  if (worker)
+    load_element_tile<N, NV, ND, NDP, EPB, NT>(M.u_in + (int64_t)e0 * NV * ND, us, ne, tid);
   __syncthreads();
 
   // ---- phase 1: node data, squared sound speed and -1/J ------------------
@@ -547,7 +557,7 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
   }
 
   // ---- phase 2a: face fluxes, one task per (element, face, face node) ------
-  for (int idx = tid; idx < ne * NFACE * NF; idx += NT) {
+  for (int idx = worker ? tid : ne * NFACE * NF; idx < ne * NFACE * NF; idx += NT) {
     // side-major task order: the lanes of a warp share the face side, so
     // they take one branch of the (own, neighbour) flux ordering
     const int side = idx >= ne * DIM * NF ? 1 : 0;
@@ -596,12 +606,15 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p) {
     const NodeFluxState<DIM> own = load_flux_state<DIM, VF>(U, P, NDP, pn);
     const double hgm1 = 0.5 * p.inv_gm1;
     node_volume_direction<0, DIM, N, VF, NDP, WARP_ALL, S::XCHG>(p, M, U, P, I, node, pn, own,
-                                                                hgm1, acc, xbuf, tid, NT);
+                                                                hgm1, acc, xbuf, tid, NT,
+                                                                worker);
     node_volume_direction<1, DIM, N, VF, NDP, WARP_ALL, S::XCHG>(p, M, U, P, I, node, pn, own,
-                                                                hgm1, acc, xbuf, tid, NT);
+                                                                hgm1, acc, xbuf, tid, NT,
+                                                                worker);
     if constexpr (DIM == 3)
       node_volume_direction<2, DIM, N, VF, NDP, WARP_ALL, S::XCHG>(p, M, U, P, I, node, pn, own,
-                                                                  hgm1, acc, xbuf, tid, NT);
+                                                                  hgm1, acc, xbuf, tid, NT,
+                                                                  worker);
     if constexpr (NS) {
       // viscous weak-form volume term sum_k Dhat(m, k) Ja^dir(k) . (-F_v)(k)
       // along each line through the node (parabolic_viscous.hpp:418-466)

@@ -161,6 +161,16 @@ class SlipWallBC:
     code = C.BC_SLIP_WALL
 
 
+class NSNoSlipAdiabaticWallBC:
+    """navier_stokes_wall_boundary.hpp:33-132 (Navier-Stokes only)."""
+    code = C.BC_NS_NOSLIP_ADIABATIC_WALL
+
+
+class NSSlipAdiabaticWallBC:
+    """navier_stokes_wall_boundary.hpp:134-219 (Navier-Stokes only)."""
+    code = C.BC_NS_SLIP_ADIABATIC_WALL
+
+
 class BoundarySet:
     """One boundary condition per face: left, right, bottom, top(, back, front)."""
 
@@ -610,6 +620,11 @@ class BatchSolver:
         C.check(C.lib().dgsem_batch_autotune(self._h, ctypes.c_void_p(u.data_ptr()), dts,
                                              chosen), "dgsem_batch_autotune")
         return list(chosen)
+
+    def set_persistent(self, enable: bool = True) -> None:
+        """One persistent launch per stage over all meshes (dgsem_batch_set_persistent)."""
+        C.check(C.lib().dgsem_batch_set_persistent(self._h, int(enable)),
+                "dgsem_batch_set_persistent")
 
     def launch_count(self) -> int:
         c = ctypes.c_int64()

@@ -81,7 +81,13 @@ typedef enum dgsem_bc_kind {
   DGSEM_BC_OUTFLOW = 2,           /* outflow_boundary.hpp:57-110 */
   DGSEM_BC_MIXED_DMR_WALL = 3,    /* MixedDirichletSlipWallBC, Dirichlet for x < 1/6 */
   DGSEM_BC_DIRICHLET_CONST = 4,   /* DirichletBC with a constant state */
-  DGSEM_BC_SLIP_WALL = 5          /* reflecting wall (MixedDirichletSlipWallBC wall branch) */
+  DGSEM_BC_SLIP_WALL = 5,         /* reflecting wall (MixedDirichletSlipWallBC wall branch) */
+  /* Navier-Stokes adiabatic walls (navier_stokes_wall_boundary.hpp): the
+   * reflected state for the inviscid flux, the wall value of the gradient
+   * variables (no-slip: zero velocity; slip: no normal velocity) for BR1, the
+   * inner viscous flux on the momentum (no-slip) or no viscous flux (slip) */
+  DGSEM_BC_NS_NOSLIP_ADIABATIC_WALL = 6,
+  DGSEM_BC_NS_SLIP_ADIABATIC_WALL = 7
 } dgsem_bc_kind;
 
 typedef enum dgsem_initial_kind {
@@ -244,6 +250,14 @@ dgsem_status dgsem_batch_check_finite(dgsem_batch* b);
 dgsem_status dgsem_batch_autotune(dgsem_batch* b, double* u, const double* dt_host,
                                   int* chosen);
 dgsem_status dgsem_batch_launch_count(const dgsem_batch* b, int64_t* count);
+/* Persistent mode (2D batches, LLF surface flux): every stage is ONE launch
+ * over the meshes of all degrees; each block of 128 threads walks a work list
+ * of (degree, element tile) items, higher degrees first, and runs that
+ * degree's node-parallel stage body.  Results agree with the per-degree
+ * launches to rounding (the same body and tiles; bit for bit where the
+ * compiler emits the same arithmetic).  DGSEM_ERR_UNSUPPORTED for other
+ * batches.  Graphs record the mode they were captured in. */
+dgsem_status dgsem_batch_set_persistent(dgsem_batch* b, int enable);
 
 /* Hennemann-Gassner blending factor per element and troubled-cell flag
  * (alpha > max(100 eps, eps^0.75), volume_flux.hpp:772-773).  Either output

@@ -46,6 +46,7 @@ enum {
   REF_EULER2D_CENTRAL_DIRICHLET = 6,  // the reference's CentralFlux + user DirichletBC
   REF_EULER2D_CURVED_CENTRAL = 7,     // curvilinear periodic mesh, CentralFlux + LLF
   REF_EULER3D_CURVED = 8,             // curvilinear periodic mesh, Chandrashekar + LLF
+  REF_NS2D_CHANNEL_WALLS = 9,         // NS, x periodic, no-slip bottom / slip top walls
 };
 
 typedef struct {
@@ -302,8 +303,12 @@ class RefCase final : public RefCaseBase {
 
   RefCase(const dgsem_ref_case& c, const Eq& eq, const Boundaries& bcs,
           bool periodic)
+      : RefCase(c, eq, bcs, make_periodic(periodic)) {}
+
+  RefCase(const dgsem_ref_case& c, const Eq& eq, const Boundaries& bcs,
+          const std::array<bool, D>& periodic)
       : mesh_(make_left(c), make_right(c), make_cells(c)),
-        solver_(eq, mesh_, container_, bcs, make_periodic(periodic)),
+        solver_(eq, mesh_, container_, bcs, periodic),
         sol_(mesh_),
         c_(c) {
     solver_.set_indicator_parameters(c.alpha_max, c.alpha_min, false);
@@ -592,6 +597,13 @@ RefCaseBase* make_case_n(const dgsem_ref_case& c) {
                                                                               map);
       }
       return nullptr;
+    }
+    case REF_NS2D_CHANNEL_WALLS: {
+      using VF = DGSEM::VolumeIntegralSplitForm<Basis, NS2, DGSEM::ChandrashekarFlux>;
+      auto b = DGSEM::BoundarySet(P{}, P{}, DGSEM::NSNoSlipAdiabaticWallBC{},
+                                  DGSEM::NSSlipAdiabaticWallBC{});
+      return new RefCase<NS2, N, VF, decltype(b), 2>(c, NS2{c.gamma, c.mu, c.prandtl}, b,
+                                                     std::array<bool, 2>{true, false});
     }
     case REF_NS2D_PERIODIC_SPLIT: {
       using VF = DGSEM::VolumeIntegralSplitForm<Basis, NS2, DGSEM::ChandrashekarFlux>;

@@ -111,3 +111,31 @@ def test_batched_autotune_keeps_results(cuda):
     # summation order only
     ua, ub = a.u.cpu().numpy(), b.u.cpu().numpy()
     assert np.max(np.abs(ua - ub)) <= 1e-13 * np.max(np.abs(ua))
+
+
+def test_persistent_launch_equals_per_degree_launches(cuda):
+    """One persistent launch per stage over all degrees (work list, 128-thread
+    blocks) against the per-degree node-parallel launches: same results to
+    rounding, every mesh; stream steps and graph replay agree bit for bit."""
+    import torch
+    a = _batch(cuda)
+    b = _batch(cuda)
+    c = _batch(cuda)
+    dts = [1.2e-3 * (1 + 0.05 * k) for k in range(len(SPECS))]
+    b.set_persistent(True)
+    c.set_persistent(True)
+    for s in range(3):
+        a.step(s * dts[0], dts)
+        b.step(s * dts[0], dts)
+    g = c.graph(dts, 3)
+    g.launch()
+    torch.cuda.synchronize()
+    b.check_finite()
+    ua, ub = a.u.cpu().numpy(), b.u.cpu().numpy()
+    assert np.isfinite(ub).all()
+    assert np.max(np.abs(ua - ub)) <= 1e-13 * np.max(np.abs(ua))
+    assert torch.equal(b.u, c.u)
+    # one launch per stage
+    n0 = b.launch_count()
+    b.step(0.0, dts)
+    assert b.launch_count() - n0 == 3
