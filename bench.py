@@ -944,7 +944,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-side-workloads", action="store_true",
                     help="skip the short batched / adjoint runs recorded in details")
-    ap.add_argument("--variant", default="auto", choices=["auto", "0", "1", "2", "3", "4", "5"],
+    ap.add_argument("--variant", default="auto", choices=["auto", "0", "1", "2", "3", "4", "5", "6"],
                     help="launch shape of the stage kernel (auto = autotuned)")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -6,7 +6,9 @@
 // for each segment, last to first, the segment's steps are recomputed from
 // its checkpoint while their stage states (u^n, u^(1), u^(2)) are kept in
 // HBM (the last segment is recorded during the forward pass and not
-// recomputed), then the adjoint SSPRK3 steps run backwards:
+// recomputed), with Navier-Stokes also the BR1 gradient of each of those
+// states as the forward stage computed it (so the reverse VJPs do not
+// recompute it), then the adjoint SSPRK3 steps run backwards:
 //   lam2 = 2/3 lam + 2/3 dt VJP(u^(2); lam)
 //   lam1 = 1/4 lam2 + 1/4 dt VJP(u^(1); lam2)
 //   lam  = 1/3 lam + 3/4 lam2 + lam1 + dt VJP(u^n; lam1)
@@ -30,12 +32,14 @@ namespace dgsem {
 class AdjointEngineBase {
  public:
   virtual ~AdjointEngineBase() = default;
-  // out = x0 X + x1 Y + b w + c (dR/du(u))^T w
-  virtual cudaError_t vjp(const EngineConfig& cfg, const double* u, const double* w,
-                          double* out, const double* X, double x0, const double* Y,
-                          double x1, double b, double c, double* xy, double* qdir,
-                          cudaStream_t s) const = 0;
-  virtual int kernels_per_vjp() const = 0;
+  // out = x0 X + x1 Y + b w + c (dR/du(u))^T w.  Navier-Stokes: `grad_u` is
+  // the forward BR1 gradient of u when the caller kept it from the forward
+  // stage; nullptr recomputes it into cfg.grad first.
+  virtual cudaError_t vjp(const EngineConfig& cfg, const double* u, const double* grad_u,
+                          const double* w, double* out, const double* X, double x0,
+                          const double* Y, double x1, double b, double c, double* xy,
+                          double* qdir, cudaStream_t s) const = 0;
+  virtual int kernels_per_vjp(bool with_gradient) const = 0;
 };
 
 template <int N, bool NS>
@@ -43,13 +47,14 @@ class AdjointEngine final : public AdjointEngineBase {
  public:
   static constexpr int EPB = (128 / (N * N)) > 0 ? (128 / (N * N)) : 1;
 
-  cudaError_t vjp(const EngineConfig& cfg, const double* u, const double* w, double* out,
-                  const double* X, double x0, const double* Y, double x1, double b,
-                  double c, double* xy, double* qdir, cudaStream_t s) const override {
+  cudaError_t vjp(const EngineConfig& cfg, const double* u, const double* grad_u,
+                  const double* w, double* out, const double* X, double x0, const double* Y,
+                  double x1, double b, double c, double* xy, double* qdir,
+                  cudaStream_t s) const override {
     AdjArgs<N> a{};
     a.u = u;
     a.w = w;
-    a.grad = cfg.grad;
+    a.grad = grad_u ? grad_u : cfg.grad;
     a.xy = xy;
     a.qdir = qdir;
     a.out = out;
@@ -82,13 +87,15 @@ class AdjointEngine final : public AdjointEngineBase {
       for (int f = 0; f < 4; ++f) ga.bc_kind[f] = 0;
       // programmatic dependent launches: each kernel's blocks are placed while
       // the previous one drains; griddepcontrol.wait orders the memory
-      launch_stage_kernel(br1_gradient_kernel<N, EPB>, blocks, EPB * N * N, 0, s, ga);
+      if (!grad_u) launch_stage_kernel(br1_gradient_kernel<N, EPB>, blocks, EPB * N * N, 0, s, ga);
       launch_stage_kernel(adj_viscous_kernel<N, EPB>, blocks, EPB * N * N, 0, s, a);
     }
     launch_stage_kernel(adj_main_kernel<N, NS, EPB>, blocks, EPB * N * N, 0, s, a);
     return cudaGetLastError();
   }
-  int kernels_per_vjp() const override { return NS ? 3 : 1; }
+  int kernels_per_vjp(bool with_gradient) const override {
+    return NS ? (with_gradient ? 3 : 2) : 1;
+  }
 };
 
 std::unique_ptr<AdjointEngineBase> make_adjoint_engine(int n, bool ns) {
@@ -228,6 +235,10 @@ struct dgsem_adjoint {
   std::vector<void*> allocations;
   double* snaps = nullptr;  // [nsnap][len]
   double* seg = nullptr;    // [every][3][len]: u^n, u^(1), u^(2) of each step
+  // Navier-Stokes: [every][3][glen] forward BR1 gradients of those states,
+  // written by the forward stages that consume them (nullptr: Euler)
+  double* gseg = nullptr;
+  int64_t glen = 0;
   double* work = nullptr;   // forward state
   double* lam = nullptr;
   double* lam2 = nullptr;
@@ -278,6 +289,22 @@ double* seg_slot(dgsem_adjoint* a, int r, int k) {
   return a->seg + ((int64_t)r * 3 + k) * a->len;
 }
 
+double* grad_slot(dgsem_adjoint* a, int r, int k) {
+  return a->gseg ? a->gseg + ((int64_t)r * 3 + k) * a->glen : nullptr;
+}
+
+// Forward stage that keeps the BR1 gradient of its input state in `gslot`
+// (the engine writes and reads the gradient through cfg.grad).
+cudaError_t fwd_stage_keep(dgsem_adjoint* a, int stage, const double* u_n, const double* u_in,
+                           double* out, double t, double dt, double* gslot) {
+  if (!gslot) return fwd_stage(a, stage, u_n, u_in, out, t, dt);
+  double* shared_grad = a->ctx->cfg.grad;
+  a->ctx->cfg.grad = gslot;
+  const cudaError_t e = fwd_stage(a, stage, u_n, u_in, out, t, dt);
+  a->ctx->cfg.grad = shared_grad;
+  return e;
+}
+
 // Steps [s0, s1) from the state in `state`, recording every step's stage
 // states in the segment buffer (slot r = s - s0); the state after s1 is
 // written back to `state`.
@@ -291,18 +318,21 @@ cudaError_t record_segment(dgsem_adjoint* a, double* state, int s0, int s1, doub
     const double t = t0 + s * dt;
     double* un = seg_slot(a, r, 0);
     double* next = (s + 1 < s1) ? seg_slot(a, r + 1, 0) : state;
-    e = fwd_stage(a, 1, nullptr, un, seg_slot(a, r, 1), t, dt);
-    if (e == cudaSuccess) e = fwd_stage(a, 2, un, seg_slot(a, r, 1), seg_slot(a, r, 2), t, dt);
-    if (e == cudaSuccess) e = fwd_stage(a, 3, un, seg_slot(a, r, 2), next, t, dt);
+    e = fwd_stage_keep(a, 1, nullptr, un, seg_slot(a, r, 1), t, dt, grad_slot(a, r, 0));
+    if (e == cudaSuccess)
+      e = fwd_stage_keep(a, 2, un, seg_slot(a, r, 1), seg_slot(a, r, 2), t, dt,
+                         grad_slot(a, r, 1));
+    if (e == cudaSuccess)
+      e = fwd_stage_keep(a, 3, un, seg_slot(a, r, 2), next, t, dt, grad_slot(a, r, 2));
   }
   return e;
 }
 
-cudaError_t launch_vjp(dgsem_adjoint* a, const double* u, const double* w, double* out,
-                       const double* X, double x0, const double* Y, double x1, double b,
-                       double c) {
-  a->ctx->launches += a->eng->kernels_per_vjp();
-  return a->eng->vjp(a->ctx->cfg, u, w, out, X, x0, Y, x1, b, c, a->xy, a->qdir,
+cudaError_t launch_vjp(dgsem_adjoint* a, const double* u, const double* grad_u,
+                       const double* w, double* out, const double* X, double x0,
+                       const double* Y, double x1, double b, double c) {
+  a->ctx->launches += a->eng->kernels_per_vjp(grad_u == nullptr);
+  return a->eng->vjp(a->ctx->cfg, u, grad_u, w, out, X, x0, Y, x1, b, c, a->xy, a->qdir,
                      a->ctx->stream);
 }
 
@@ -358,7 +388,9 @@ dgsem_status dgsem_adjoint_create(dgsem_ctx* ctx, int nsteps, int checkpoint_eve
   if (a->work) a->lam = adj_alloc(a, a->len, &err);
   if (a->lam) a->lam2 = adj_alloc(a, a->len, &err);
   if (a->lam2) a->lam1 = adj_alloc(a, a->len, &err);
-  if (a->lam1) a->xy = adj_alloc(a, ns ? (size_t)nodes * 8 : 1, &err);
+  a->glen = ns ? nodes * 8 : 0;
+  if (a->lam1 && ns) a->gseg = adj_alloc(a, (size_t)a->every * 3 * a->glen, &err);
+  if (a->lam1 && (!ns || a->gseg)) a->xy = adj_alloc(a, ns ? (size_t)nodes * 8 : 1, &err);
   if (a->xy) a->qdir = adj_alloc(a, ns ? (size_t)nodes * 2 : 1, &err);
   if (a->qdir) a->partial = adj_alloc(a, (size_t)a->ke_blocks * 2, &err);
   if (a->partial) a->result = adj_alloc(a, 2, &err);
@@ -390,7 +422,7 @@ dgsem_status dgsem_adjoint_destroy(dgsem_adjoint* a) {
 dgsem_status dgsem_adjoint_rhs_vjp(dgsem_adjoint* a, const double* u, const double* w,
                                    double* out) {
   if (!a || !u || !w || !out || out == w) return DGSEM_ERR_INVALID_ARG;
-  return st_of(launch_vjp(a, u, w, out, nullptr, 0.0, nullptr, 0.0, 0.0, 1.0));
+  return st_of(launch_vjp(a, u, nullptr, w, out, nullptr, 0.0, nullptr, 0.0, 0.0, 1.0));
 }
 
 dgsem_status dgsem_kinetic_energy(dgsem_adjoint* a, const double* u, double* value,
@@ -445,14 +477,14 @@ dgsem_status dgsem_adjoint_gradient(dgsem_adjoint* a, const double* u0, double t
     }
     for (int s = s1 - 1; s >= s0 && e == cudaSuccess; --s) {
       const int r = s - s0;
-      e = launch_vjp(a, seg_slot(a, r, 2), a->lam, a->lam2, nullptr, 0.0, nullptr, 0.0,
-                     2.0 / 3.0, (2.0 / 3.0) * dt);
+      e = launch_vjp(a, seg_slot(a, r, 2), grad_slot(a, r, 2), a->lam, a->lam2, nullptr, 0.0,
+                     nullptr, 0.0, 2.0 / 3.0, (2.0 / 3.0) * dt);
       if (e == cudaSuccess)
-        e = launch_vjp(a, seg_slot(a, r, 1), a->lam2, a->lam1, nullptr, 0.0, nullptr, 0.0,
-                       1.0 / 4.0, (1.0 / 4.0) * dt);
+        e = launch_vjp(a, seg_slot(a, r, 1), grad_slot(a, r, 1), a->lam2, a->lam1, nullptr,
+                       0.0, nullptr, 0.0, 1.0 / 4.0, (1.0 / 4.0) * dt);
       if (e == cudaSuccess)
-        e = launch_vjp(a, seg_slot(a, r, 0), a->lam1, a->lam, a->lam, 1.0 / 3.0, a->lam2,
-                       3.0 / 4.0, 1.0, dt);
+        e = launch_vjp(a, seg_slot(a, r, 0), grad_slot(a, r, 0), a->lam1, a->lam, a->lam,
+                       1.0 / 3.0, a->lam2, 3.0 / 4.0, 1.0, dt);
     }
   }
   if (e == cudaSuccess)

@@ -14,6 +14,7 @@
 
 #include "br1_kernel.cuh"
 #include "stage_kernel.cuh"
+#include "stage_node2_kernel.cuh"
 #include "stage_node_kernel.cuh"
 #include "stage_pipe_kernel.cuh"
 #include "tables.hpp"
@@ -46,7 +47,7 @@ struct EngineConfig {
 // tile streaming (stage_pipe_kernel.cuh; single-mesh launches).  3-5 cover
 // the split form without shock capturing or viscous terms; 5 needs an even
 // number of doubles per element (2D, or 3D with even n).
-constexpr int kNumVariants = 6;
+constexpr int kNumVariants = 7;
 
 class EngineBase {
  public:
@@ -248,6 +249,24 @@ class Engine final : public EngineBase {
                           args);
   }
 
+  // shape 6: two nodes per thread (3D, n = 2 or 4, split form)
+  static constexpr bool kNode2 = DIM == 3 && (N == 2 || N == 4) && !HG && !NS;
+  template <int NN = N>
+  static auto node2_kernel() {
+    return stage_node2_kernel<NN, VF, SF>;
+  }
+  void launch_node2(const StageArgs<N>& args, int64_t nelem, cudaStream_t s) const {
+    if constexpr (kNode2) {
+      using S2 = Node2Shape<N, VF>;
+      const int64_t blocks = (nelem + Node2Launch<N>::EPB - 1) / Node2Launch<N>::EPB;
+      last_grid_ = blocks;
+      launch_stage_kernel(node2_kernel(), (unsigned)blocks, Node2Launch<N>::NT,
+                          args.a != 0.0 ? S2::smem_bytes : S2::smem_bytes_base, s, args);
+    } else {
+      launch_node<true>(args, nelem, s);
+    }
+  }
+
   using PSh = PipeShape<DIM, N, VF, NL::EPB>;
   static constexpr bool kPipe = kBatch && PSh::kSupported;
   static auto pipe_kernel() {
@@ -299,6 +318,9 @@ class Engine final : public EngineBase {
     if constexpr (kPipe)
       cudaFuncSetAttribute(pipe_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)PSh::smem_bytes);
+    if constexpr (kNode2)
+      cudaFuncSetAttribute(node2_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)Node2Shape<N, VF>::smem_bytes);
   }
 
   StageArgs<N> common_args(const EngineConfig& cfg, double a, double b, double t,
@@ -355,6 +377,7 @@ class Engine final : public EngineBase {
       case 3: launch_node<true>(args, cfg.nelem, s); break;
       case 4: launch_node<false>(args, cfg.nelem, s); break;
       case 5: launch_pipe(args, cfg.nelem, s); break;
+      case 6: launch_node2(args, cfg.nelem, s); break;
       default: launch<0>(args, cfg.nelem, s); break;
     }
     if (diag) last_diag_slots_ = last_grid_;
@@ -384,7 +407,8 @@ class Engine final : public EngineBase {
         case 1: launch_batch<1>(args, ntiles, s); break;
         case 2: launch_batch<2>(args, ntiles, s); break;
         case 3:
-        case 5: launch_node_batch<true>(args, ntiles, s); break;
+        case 5:
+        case 6: launch_node_batch<true>(args, ntiles, s); break;
         case 4: launch_node_batch<false>(args, ntiles, s); break;
         default: launch_batch<0>(args, ntiles, s); break;
       }
@@ -395,6 +419,8 @@ class Engine final : public EngineBase {
   int kernels_per_stage() const override { return NS ? 2 : 1; }
   int64_t last_diag_slots() const override { return last_diag_slots_; }
   int elements_per_block() const override {
+    if constexpr (kNode2)
+      if (variant_ == 6) return Node2Launch<N>::EPB;
     if (variant_ >= 3 || !kLine) return NL::EPB;
     return variant_ == 2 ? LaunchShape<DIM, N, 2>::EPB : LaunchShape<DIM, N, 0>::EPB;
   }
@@ -403,13 +429,15 @@ class Engine final : public EngineBase {
     return variant_ == 2 ? LaunchShape<DIM, N, 2>::NT : LaunchShape<DIM, N, 0>::NT;
   }
   size_t smem_bytes() const override {
+    if constexpr (kNode2)
+      if (variant_ == 6) return Node2Shape<N, VF>::smem_bytes;
     if (variant_ >= 3 || !kLine) return NSh::smem_bytes;
     return variant_ == 2 ? Sh<2>::smem_bytes : Sh<0>::smem_bytes;
   }
   void set_variant(int v) override { variant_ = (v >= 0 && v < num_variants()) ? v : 0; }
   int variant() const override { return variant_; }
-  // shape 5 exists for single-mesh launches; batched launches run it as 3
-  int num_variants() const override { return kPipe ? 6 : kNode ? 5 : 3; }
+  // shapes 5 and 6 exist for single-mesh launches; batched launches run them as 3
+  int num_variants() const override { return kNode2 ? 7 : kPipe ? 6 : kNode ? 5 : 3; }
 
  private:
   int variant_ = 0;

@@ -28,6 +28,7 @@ struct NodeState {
   double p;
   double beta;  // 0.5 rho / p  (Chandrashekar); e = E / rho (Kennedy-Gruber)
   double kin;   // 0.5 |v|^2
+  double inv_rho;
 };
 
 // Logarithmic mean and its inverse with the reference's branch rule
@@ -83,6 +84,7 @@ __device__ __forceinline__ NodeState<DIM> prepare_node(const double* u,
   NodeState<DIM> s;
   s.rho = u[0];
   const double inv_rho = 1.0 / u[0];
+  s.inv_rho = inv_rho;
   double sq = 0.0;
 #pragma unroll
   for (int d = 0; d < DIM; ++d) {

@@ -8,7 +8,7 @@
 //   1  per-node flux data (NodeKernelSlots), squared sound speed and -1/J;
 //   2a face tasks: every (face, face node) of the block's elements computes
 //      its interface / boundary flux f* once into a shared face buffer
-//      (tasks ordered side-major, so a warp's lanes share the face side and
+//      (tasks grouped by side and direction, so a warp's lanes share both and
 //      evaluate the flux in one argument order);
 //   2b one thread per node: for each direction, the two-point fluxes with the
 //      n-1 other nodes of its line, sum_k Dsplit(m, k) f(u_m, u_k, (Ja_m +
@@ -342,6 +342,146 @@ __device__ __forceinline__ void node_fv_direction(const StageArgs<N>& p, const M
 // NTB: threads of the launch (>= EPB * n^d; the threads past EPB * n^d only
 // take part in the block's barriers).  PERSIST: batched launches whose
 // tiles come from a work list (`tile`), without the bulk copy of u_n.
+// Element info of a tile, info[el * NI + entry]: 0-2 the element's indices,
+// 3-5 its row in the metric tables of each axis (the indices of the other
+// axes), 6.. the neighbour across each face (-1 at a boundary face; unused
+// entries -1).  One entry per thread, so the whole tile's info is one pass
+// of ne * NI threads instead of a serial loop per element.
+template <int DIM, int NI>
+__device__ __forceinline__ void node_element_info(const MeshView& M, int* info, int e0, int ne,
+                                                  int tid, int nt) {
+  const int c0 = M.cells[0], c1 = M.cells[1], c2 = M.cells[2];
+  for (int k = tid; k < ne * NI; k += nt) {
+    const int el = k / NI, entry = k - el * NI;
+    const int e = e0 + el;
+    const int i0 = e % c0;
+    const int i1 = DIM == 2 ? e / c0 : (e / c0) % c1;
+    const int i2 = DIM == 2 ? 0 : e / (c0 * c1);
+    int v = -1;
+    if (entry == 0) v = i0;
+    else if (entry == 1) v = i1;
+    else if (entry == 2) v = i2;
+    else if (entry == 3) v = DIM == 2 ? i1 : i1 + c1 * i2;
+    else if (entry == 4) v = DIM == 2 ? i0 : i0 + c0 * i2;
+    else if (entry == 5) v = DIM == 2 ? 0 : i0 + c0 * i1;
+    else if (entry < 6 + 2 * DIM) {
+      const int face = entry - 6, dir = face >> 1;
+      const int id = dir == 0 ? i0 : dir == 1 ? i1 : i2;
+      const int cd = dir == 0 ? c0 : dir == 1 ? c1 : c2;
+      const int stride = dir == 0 ? 1 : dir == 1 ? c0 : c0 * c1;
+      int pos = id + ((face & 1) ? 1 : -1);
+      if (pos < 0 || pos >= cd) pos = M.periodic[dir] ? (pos + cd) % cd : -1;
+      v = pos < 0 ? -1 : e + (pos - id) * stride;
+    }
+    info[k] = v;
+  }
+}
+
+// Per-node data of phase 1 (NodeKernelSlots) from the conserved state u:
+// the (halved) primitive variables, the squared sound speed gamma p / rho and
+// -1/J from the separable metric tables.
+template <int DIM, int N, int VF, int NDP>
+__device__ __forceinline__ void node_prepare(const MeshView& M, const double* u, double gamma,
+                                             const int* I, int node, double* P) {
+  using K = NodeKernelSlots<DIM, VF>;
+  const NodeState<DIM> s = prepare_node<DIM, VF>(u, gamma);
+  const double h = K::HALF ? 0.5 : 1.0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) P[(K::V + d) * NDP] = h * s.v[d];
+  P[K::P * NDP] = h * s.p;
+  // used only by the wave-speed estimate of the surface flux: gamma p (1/rho)
+  // is within an ulp of gamma p / rho
+  P[K::A * NDP] = gamma * s.p * s.inv_rho;
+  if constexpr (K::HALF) {
+    P[K::H_RHO * NDP] = 0.5 * u[0];
+    P[K::X * NDP] = VF == VF_KENNEDY_GRUBER ? 0.5 * s.beta : s.beta;
+  }
+  if constexpr (VF == VF_CHANDRASHEKAR) P[K::Y * NDP] = 0.5 * s.kin;
+  const int in = node % N, jn = (node / N) % N, kn = DIM == 3 ? node / (N * N) : 0;
+  double jdet = __ldg(M.tab.jdiag[0] + I[0] * N + in);
+  if (DIM == 2) {
+    jdet = jdet * __ldg(M.tab.jdiag[1] + I[1] * N + jn);
+  } else {
+    jdet = jdet * (__ldg(M.tab.jdiag[1] + I[1] * N + jn) * __ldg(M.tab.jdiag[2] + I[2] * N + kn));
+  }
+  P[K::MIJ * NDP] = -(1.0 / jdet);
+}
+
+// Surface lifting of one node (surface_integral.hpp:35-154): per direction,
+// -lhat_l0 f* of the low face or +lhat_rN f* of the high face when the node
+// lies on it.  Branch-free: every node reads one face flux per direction and
+// interior nodes add it with the factor 0 (acc + 0 f = acc), so the lanes of
+// a warp do not diverge over the faces.  sf_el = face buffer of the element.
+template <int DIM, int N>
+__device__ __forceinline__ void node_lift(const double* sf_el, int node, double lhat_l0,
+                                          double lhat_rN, double* acc) {
+  constexpr int NV = DIM + 2, NF = ipow(N, DIM - 1);
+  const int pos[3] = {node % N, (node / N) % N, DIM == 3 ? node / (N * N) : 0};
+#pragma unroll
+  for (int dir = 0; dir < DIM; ++dir) {
+    const int line = dir == 0   ? node / N
+                     : dir == 1 ? node % N + N * (node / (N * N))
+                                : node % (N * N);
+    const bool hi = pos[dir] == N - 1;
+    const double coef = pos[dir] == 0 ? -lhat_l0 : hi ? lhat_rN : 0.0;
+    const double* F = sf_el + ((2 * dir + (hi ? 1 : 0)) * NF + line) * NV;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) acc[q] += coef * F[q];
+  }
+}
+
+// Phase 2a of the node-parallel kernels: the interface / boundary flux f* of
+// every (element, face, face node) of the tile, once, into the face buffer
+// sf[el][face][fn][var].  Tasks are grouped by (side, direction), both
+// compile-time constants in the flux code (no runtime-indexed arrays);
+// inside a group the order is element-major, and a group fills whole warps
+// where ne * NF is a multiple of 32, so a warp's lanes share the face side
+// and direction and evaluate the flux in one argument order.  Task idx of
+// the tile goes to thread idx % NT, as in one block-stride loop.
+template <int DIM, int N, int VF, int SF, bool NS, int NDP, int NT, int NQ, int NI>
+__device__ __forceinline__ void node_face_tasks(const StageArgs<N>& p, const MeshView& M,
+                                                const double* us, const double* pr,
+                                                const double* wv, const int* info, double* sf,
+                                                int ne, int tid, double gamma, double t_stage,
+                                                int c0, int c1, int c2) {
+  using K = NodeKernelSlots<DIM, VF>;
+  constexpr int NV = DIM + 2, ND = ipow(N, DIM), NF = ipow(N, DIM - 1), NFACE = 2 * DIM;
+  const int gsz = ne * NF;
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+#pragma unroll
+    for (int dir = 0; dir < DIM; ++dir) {
+      const int gbase = (side * DIM + dir) * gsz;
+      int r = tid - gbase % NT;
+      if (r < 0) r += NT;
+      for (; r < gsz; r += NT) {
+        const int fe = r / NF, fn = r - (r / NF) * NF;
+        const int face = 2 * dir + side;
+        const int* I = info + fe * NI;
+        const double* U = us + fe * NV * NDP;
+        const double* P = pr + fe * NQ * NDP;
+        const int opn = padn<N, NDP != ND>(line_node<DIM, N>(dir, fn, side ? N - 1 : 0));
+        FaceState<DIM> so;
+#pragma unroll
+        for (int q = 0; q < NV; ++q) so.u[q] = U[q * NDP + opn];
+        const double g = K::HALF ? 2.0 : 1.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) so.v[d] = g * P[(K::V + d) * NDP + opn];
+        so.p = g * P[K::P * NDP + opn];
+        so.a2 = P[K::A * NDP + opn];
+        double f[NV];
+        element_face_flux_state<DIM, N, VF, SF, NS, NDP>(p, M, so, U,
+                                                         NS ? wv + fe * 2 * NV * ND : nullptr,
+                                                         I, dir, side, fn, gamma, t_stage, c0,
+                                                         c1, c2, f);
+        double* F = sf + ((fe * NFACE + face) * NF + fn) * NV;
+#pragma unroll
+        for (int q = 0; q < NV; ++q) F[q] = f[q];
+      }
+    }
+  }
+}
+
 template <int DIM, int N, int VF, int SF, int EPB, bool BATCH, bool HG, bool NS = false,
           int NTB = 0, bool PERSIST = false>
 __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile = 0) {
@@ -399,43 +539,7 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile 
   }
 
   // ---- phase 0: element info and the u_in tile --------------------------
-  for (int el = tid; el < ne; el += NT) {
-    const int e = e0 + el;
-    int ijk[3];
-    ijk[0] = e % c0;
-    ijk[1] = DIM == 2 ? e / c0 : (e / c0) % c1;
-    ijk[2] = DIM == 2 ? 0 : e / (c0 * c1);
-    int* I = info + el * NI;
-    I[0] = ijk[0];
-    I[1] = ijk[1];
-    I[2] = ijk[2];
-    if (DIM == 2) {
-      I[3] = ijk[1];
-      I[4] = ijk[0];
-      I[5] = 0;
-    } else {
-      I[3] = ijk[1] + c1 * ijk[2];
-      I[4] = ijk[0] + c0 * ijk[2];
-      I[5] = ijk[0] + c0 * ijk[1];
-    }
-    const int cells[3] = {c0, c1, c2};
-#pragma unroll
-    for (int face = 0; face < NFACE; ++face) {
-      const int dir = face >> 1, side = face & 1;
-      int pos = ijk[dir] + (side ? 1 : -1);
-      int nbr = -1;
-      if (pos < 0 || pos >= cells[dir]) {
-        if (M.periodic[dir]) pos = (pos + cells[dir]) % cells[dir];
-        else pos = -1;
-      }
-      if (pos >= 0) {
-        int q[3] = {ijk[0], ijk[1], ijk[2]};
-        q[dir] = pos;
-        nbr = DIM == 2 ? q[0] + c0 * q[1] : q[0] + c0 * (q[1] + c1 * q[2]);
-      }
-      I[6 + face] = nbr;
-    }
-  }
+  node_element_info<DIM, NI>(M, info, e0, ne, tid, NT);
   if constexpr (HG) {
     for (int k = tid; k < N * N; k += NT) vinv_s[k] = p.basis.Vinv[k / N][k % N];
   }
@@ -451,27 +555,7 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile 
     double u[NV];
 #pragma unroll
     for (int q = 0; q < NV; ++q) u[q] = us[(el * NV + q) * NDP + pn];
-    const NodeState<DIM> s = prepare_node<DIM, VF>(u, gamma);
-    double* P = pr + el * NQ * NDP + pn;
-    const double h = K::HALF ? 0.5 : 1.0;
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) P[(K::V + d) * NDP] = h * s.v[d];
-    P[K::P * NDP] = h * s.p;
-    P[K::A * NDP] = gamma * s.p / u[0];
-    if constexpr (K::HALF) {
-      P[K::H_RHO * NDP] = 0.5 * u[0];
-      P[K::X * NDP] = VF == VF_KENNEDY_GRUBER ? 0.5 * s.beta : s.beta;
-    }
-    if constexpr (VF == VF_CHANDRASHEKAR) P[K::Y * NDP] = 0.5 * s.kin;
-    const int* I = info + el * NI;
-    const int in = node % N, jn = (node / N) % N, kn = DIM == 3 ? node / (N * N) : 0;
-    double jdet = __ldg(M.tab.jdiag[0] + I[0] * N + in);
-    if (DIM == 2) {
-      jdet = jdet * __ldg(M.tab.jdiag[1] + I[1] * N + jn);
-    } else {
-      jdet = jdet * (__ldg(M.tab.jdiag[1] + I[1] * N + jn) * __ldg(M.tab.jdiag[2] + I[2] * N + kn));
-    }
-    P[K::MIJ * NDP] = -(1.0 / jdet);
+    node_prepare<DIM, N, VF, NDP>(M, u, gamma, info + el * NI, node, pr + el * NQ * NDP + pn);
     if constexpr (NS) {
       // -F_v at the node from the lifted gradient (parabolic_viscous.hpp:358-396)
       double q[4], gx[4], gy[4];
@@ -557,36 +641,9 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile 
   }
 
   // ---- phase 2a: face fluxes, one task per (element, face, face node) ------
-  for (int idx = worker ? tid : ne * NFACE * NF; idx < ne * NFACE * NF; idx += NT) {
-    // side-major task order: the lanes of a warp share the face side, so
-    // they take one branch of the (own, neighbour) flux ordering
-    const int side = idx >= ne * DIM * NF ? 1 : 0;
-    const int r = idx - side * ne * DIM * NF;
-    const int fe = r / (DIM * NF);
-    const int dir = (r / NF) % DIM;
-    const int fn = r % NF;
-    const int face = 2 * dir + side;
-    const int* I = info + fe * NI;
-    const double* U = us + fe * NV * NDP;
-    const double* P = pr + fe * NQ * NDP;
-    const int opn = padn<N, S::PAD>(line_node<DIM, N>(dir, fn, side ? N - 1 : 0));
-    FaceState<DIM> so;
-#pragma unroll
-    for (int q = 0; q < NV; ++q) so.u[q] = U[q * NDP + opn];
-    const double g = K::HALF ? 2.0 : 1.0;
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) so.v[d] = g * P[(K::V + d) * NDP + opn];
-    so.p = g * P[K::P * NDP + opn];
-    so.a2 = P[K::A * NDP + opn];
-    double f[NV];
-    element_face_flux_state<DIM, N, VF, SF, NS, NDP>(p, M, so, U,
-                                                     NS ? wv + fe * 2 * NV * ND : nullptr, I,
-                                                     dir, side, fn, gamma, t_stage, c0, c1, c2,
-                                                     f);
-    double* F = sf + ((fe * NFACE + face) * NF + fn) * NV;
-#pragma unroll
-    for (int q = 0; q < NV; ++q) F[q] = f[q];
-  }
+  if (worker)
+    node_face_tasks<DIM, N, VF, SF, NS, NDP, NT, NQ, NI>(p, M, us, pr, wv, info, sf, ne, tid,
+                                                         gamma, t_stage, c0, c1, c2);
 
   // ---- phase 2b: volume term, one thread per node --------------------------
   double acc[NV];
@@ -668,25 +725,7 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile 
   if (active) {
 
   // ---- phase 3: lifting (surface_integral.hpp:35-154), -1/J, SSPRK3 --------
-  {
-    const int pos[3] = {node % N, (node / N) % N, DIM == 3 ? node / (N * N) : 0};
-#pragma unroll
-    for (int dir = 0; dir < DIM; ++dir) {
-      const int line = dir == 0 ? node / N
-                       : dir == 1 ? node % N + N * (node / (N * N))
-                                  : node % (N * N);
-      if (pos[dir] == 0) {
-        const double* F = sf + ((el * NFACE + 2 * dir) * NF + line) * NV;
-#pragma unroll
-        for (int q = 0; q < NV; ++q) acc[q] -= F[q] * p.basis.lhat_l0;
-      }
-      if (pos[dir] == N - 1) {
-        const double* F = sf + ((el * NFACE + 2 * dir + 1) * NF + line) * NV;
-#pragma unroll
-        for (int q = 0; q < NV; ++q) acc[q] += F[q] * p.basis.lhat_rN;
-      }
-    }
-  }
+  node_lift<DIM, N>(sf + el * NFACE * NF * NV, node, p.basis.lhat_l0, p.basis.lhat_rN, acc);
   const double mij = pr[(el * NQ + K::MIJ) * NDP + pn];
   const int64_t gbase = (int64_t)(e0 + el) * NV * ND + node;
   bool bad = false;

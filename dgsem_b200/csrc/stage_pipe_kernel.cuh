@@ -97,43 +97,7 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
     const bool active = el < ne;
 
     // ---- element info ------------------------------------------------------
-    if (tid < ne) {
-      const int e = e0 + tid;
-      int ijk[3];
-      ijk[0] = e % c0;
-      ijk[1] = DIM == 2 ? e / c0 : (e / c0) % c1;
-      ijk[2] = DIM == 2 ? 0 : e / (c0 * c1);
-      int* I = info + tid * NI;
-      I[0] = ijk[0];
-      I[1] = ijk[1];
-      I[2] = ijk[2];
-      if (DIM == 2) {
-        I[3] = ijk[1];
-        I[4] = ijk[0];
-        I[5] = 0;
-      } else {
-        I[3] = ijk[1] + c1 * ijk[2];
-        I[4] = ijk[0] + c0 * ijk[2];
-        I[5] = ijk[0] + c0 * ijk[1];
-      }
-      const int cells[3] = {c0, c1, c2};
-#pragma unroll
-      for (int face = 0; face < NFACE; ++face) {
-        const int dir = face >> 1, side = face & 1;
-        int pos = ijk[dir] + (side ? 1 : -1);
-        int nbr = -1;
-        if (pos < 0 || pos >= cells[dir]) {
-          if (M.periodic[dir]) pos = (pos + cells[dir]) % cells[dir];
-          else pos = -1;
-        }
-        if (pos >= 0) {
-          int q[3] = {ijk[0], ijk[1], ijk[2]};
-          q[dir] = pos;
-          nbr = DIM == 2 ? q[0] + c0 * q[1] : q[0] + c0 * (q[1] + c1 * q[2]);
-        }
-        I[6 + face] = nbr;
-      }
-    }
+    node_element_info<DIM, NI>(M, info, e0, ne, tid, NT);
     // the block agrees on a timeout (vote) so that all of it leaves together
     if (__syncthreads_or(!mbar_wait_bounded(&bar_in, phase, p.wait_limit_ns))) {
       if (tid == 0) atomicOr(p.nonfinite, 2u);
@@ -148,28 +112,7 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
         u[q] = stage_in[(el * NV + q) * ND + node];
         us[(el * NV + q) * NDP + pn] = u[q];
       }
-      const NodeState<DIM> s = prepare_node<DIM, VF>(u, gamma);
-      double* P = pr + el * NQ * NDP + pn;
-      const double h = K::HALF ? 0.5 : 1.0;
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) P[(K::V + d) * NDP] = h * s.v[d];
-      P[K::P * NDP] = h * s.p;
-      P[K::A * NDP] = gamma * s.p / u[0];
-      if constexpr (K::HALF) {
-        P[K::H_RHO * NDP] = 0.5 * u[0];
-        P[K::X * NDP] = VF == VF_KENNEDY_GRUBER ? 0.5 * s.beta : s.beta;
-      }
-      if constexpr (VF == VF_CHANDRASHEKAR) P[K::Y * NDP] = 0.5 * s.kin;
-      const int* I = info + el * NI;
-      const int in = node % N, jn = (node / N) % N, kn = DIM == 3 ? node / (N * N) : 0;
-      double jdet = __ldg(M.tab.jdiag[0] + I[0] * N + in);
-      if (DIM == 2) {
-        jdet = jdet * __ldg(M.tab.jdiag[1] + I[1] * N + jn);
-      } else {
-        jdet = jdet * (__ldg(M.tab.jdiag[1] + I[1] * N + jn) *
-                       __ldg(M.tab.jdiag[2] + I[2] * N + kn));
-      }
-      P[K::MIJ * NDP] = -(1.0 / jdet);
+      node_prepare<DIM, N, VF, NDP>(M, u, gamma, info + el * NI, node, pr + el * NQ * NDP + pn);
     }
     __syncthreads();
     // stage_in is consumed: request the next tile's u_in
@@ -177,34 +120,8 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
       request(&bar_in, stage_in, M.u_in, t + gridDim.x);
 
     // ---- phase 2a: face fluxes ---------------------------------------------
-    for (int idx = tid; idx < ne * NFACE * NF; idx += NT) {
-      // side-major task order: the lanes of a warp share the face side, so
-      // they take one branch of the (own, neighbour) flux ordering
-      const int side = idx >= ne * DIM * NF ? 1 : 0;
-      const int r = idx - side * ne * DIM * NF;
-      const int fe = r / (DIM * NF);
-      const int dir = (r / NF) % DIM;
-      const int fn = r % NF;
-      const int face = 2 * dir + side;
-      const int* I = info + fe * NI;
-      const double* U = us + fe * NV * NDP;
-      const double* P = pr + fe * NQ * NDP;
-      const int opn = padn<N, S::B::PAD>(line_node<DIM, N>(dir, fn, side ? N - 1 : 0));
-      FaceState<DIM> so;
-#pragma unroll
-      for (int q = 0; q < NV; ++q) so.u[q] = U[q * NDP + opn];
-      const double g = K::HALF ? 2.0 : 1.0;
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) so.v[d] = g * P[(K::V + d) * NDP + opn];
-      so.p = g * P[K::P * NDP + opn];
-      so.a2 = P[K::A * NDP + opn];
-      double f[NV];
-      element_face_flux_state<DIM, N, VF, SF, false, NDP>(p, M, so, U, nullptr, I, dir, side, fn,
-                                                          gamma, t_stage, c0, c1, c2, f);
-      double* F = sf + ((fe * NFACE + face) * NF + fn) * NV;
-#pragma unroll
-      for (int q = 0; q < NV; ++q) F[q] = f[q];
-    }
+    node_face_tasks<DIM, N, VF, SF, false, NDP, NT, NQ, NI>(p, M, us, pr, nullptr, info, sf, ne,
+                                                            tid, gamma, t_stage, c0, c1, c2);
 
     // ---- phase 2b: volume term ---------------------------------------------
     double acc[NV];
@@ -237,23 +154,7 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
       return;
     }
     if (active) {
-      const int pos[3] = {node % N, (node / N) % N, DIM == 3 ? node / (N * N) : 0};
-#pragma unroll
-      for (int dir = 0; dir < DIM; ++dir) {
-        const int line = dir == 0 ? node / N
-                         : dir == 1 ? node % N + N * (node / (N * N))
-                                    : node % (N * N);
-        if (pos[dir] == 0) {
-          const double* F = sf + ((el * NFACE + 2 * dir) * NF + line) * NV;
-#pragma unroll
-          for (int q = 0; q < NV; ++q) acc[q] -= F[q] * p.basis.lhat_l0;
-        }
-        if (pos[dir] == N - 1) {
-          const double* F = sf + ((el * NFACE + 2 * dir + 1) * NF + line) * NV;
-#pragma unroll
-          for (int q = 0; q < NV; ++q) acc[q] += F[q] * p.basis.lhat_rN;
-        }
-      }
+      node_lift<DIM, N>(sf + el * NFACE * NF * NV, node, p.basis.lhat_l0, p.basis.lhat_rN, acc);
       const double mij = pr[(el * NQ + K::MIJ) * NDP + pn];
       const int64_t gbase = (int64_t)(e0 + el) * NV * ND + node;
       bool bad = false;

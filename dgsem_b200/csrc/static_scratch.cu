@@ -82,3 +82,18 @@ extern "C" dgsem_status dgsem_ssprk3_step_static_scratch(dgsem_ctx* ctx, double*
   if (st == DGSEM_OK) st = dgsem_ssprk3_stage(ctx, 3, u, s2, u, t, dt);
   return st;
 }
+
+extern "C" dgsem_status dgsem_static_scratch_state(int k, const double** out) {
+  if (!out || k < 0 || k > 1) return DGSEM_ERR_INVALID_ARG;
+  *out = nullptr;
+  int device = -1;
+  if (cudaGetDevice(&device) != cudaSuccess) {
+    cudaGetLastError();
+    return DGSEM_ERR_CUDA;
+  }
+  double* scratch = nullptr;
+  const dgsem_status st = scratch_on_device(device, &scratch);
+  if (st != DGSEM_OK) return st;
+  *out = scratch + (int64_t)k * DGSEM_STATIC_SCRATCH_MAX_STATE;
+  return DGSEM_OK;
+}

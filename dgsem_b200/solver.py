@@ -352,7 +352,7 @@ class StructuredSolver:
         """Picks the fastest launch shape for this mesh (results are identical
         across shapes); returns (variant, per-variant ms or None)."""
         chosen = ctypes.c_int()
-        times = (ctypes.c_double * 6)() if retime else None
+        times = (ctypes.c_double * 7)() if retime else None
         C.check(C.lib().dgsem_autotune(self._ctx, _ptr(u), ctypes.byref(chosen), times),
                 "dgsem_autotune")
         return chosen.value, (list(times) if retime else None)

@@ -197,6 +197,12 @@ dgsem_status dgsem_ssprk3_steps(dgsem_ctx* ctx, double* u, double t0,
 dgsem_status dgsem_ssprk3_step_static_scratch(dgsem_ctx* ctx, double* u,
                                               double t, double dt);
 
+/* Device address of stage state k (0: u^(1), 1: u^(2)) of the static scratch
+ * on the current device, for inspection: after a
+ * dgsem_ssprk3_step_static_scratch call has completed it holds that step's
+ * stage state in its first state_len doubles.  Read-only for the caller. */
+dgsem_status dgsem_static_scratch_state(int k, const double** out);
+
 /* nsteps SSPRK3 steps on a HOST array (the reference's host-side view of
  * the state): copies u_host to the device, steps, copies back and
  * synchronises.  u_host should be pinned for full copy bandwidth. */
@@ -284,12 +290,12 @@ dgsem_status dgsem_from_reference_layout(dgsem_ctx* ctx, const double* u_ref,
 dgsem_status dgsem_check_finite(dgsem_ctx* ctx);
 
 /* Launch-shape autotuner (no reference counterpart; the reference has one
- * fixed Kokkos launch shape).  The fused stage kernel has up to 6 launch
+ * fixed Kokkos launch shape).  The fused stage kernel has up to 7 launch
  * shapes: 0-2 line-parallel (elements per block, register cap), 3-4
- * node-parallel with and without a register cap (split form with or without
- * shock capturing, not Navier-Stokes), 5 persistent node-parallel streaming
- * element tiles through shared memory with bulk copies (no shock capturing;
- * 2D or even n in 3D).  The shapes of each group run the same source: their
+ * node-parallel with and without a register cap, 5 persistent node-parallel
+ * streaming element tiles through shared memory with bulk copies (no shock
+ * capturing or viscous terms; 2D or even n in 3D), 6 node-parallel with two
+ * nodes per thread (3D, n = 2 or 4, no shock capturing or viscous terms).  The shapes of each group run the same source: their
  * results agree bit for bit where the compiler emits the same arithmetic and
  * to rounding where a register cap changes which multiply-adds it fuses
  * (seen between 3 and 4 at n = 7 with the Ranocha flux); 3-5 agree with 0-2
@@ -298,7 +304,7 @@ dgsem_status dgsem_check_finite(dgsem_ctx* ctx);
  * one SSPRK3 step from state u (into the context temporaries; u is not
  * modified) with each available shape, 7 times in rounds that visit the
  * shapes in rotated order, keeps the one with the smallest median and returns
- * it in *chosen (may be NULL); times_ms (6 doubles, may be NULL; 0 for an
+ * it in *chosen (may be NULL); times_ms (7 doubles, may be NULL; 0 for an
  * unavailable shape) receives the median step times and forces re-timing.
  * Every timed step is preceded by an L2 eviction (a 256 MiB temporary
  * buffer, freed before returning), i.e. states stream from HBM as in large

@@ -63,7 +63,7 @@ def test_fused_diagnostics_match_oracle(name, cuda):
     # diagnostics off: reference trajectory
     C.check(L.dgsem_ssprk3_steps(solver.handle, p(ref), 0.0, c["dt"], 3), "steps")
     C.check(L.dgsem_set_diagnostics(solver.handle, 1), "enable")
-    for v in range(6):
+    for v in range(7):
         if L.dgsem_set_launch_variant(solver.handle, v) != C.DGSEM_OK:
             continue  # shape not available for this scheme
         sol.u.copy_(u0)

@@ -48,7 +48,7 @@ def test_node_shapes_every_degree(case, cuda):
     nd = case["ndims"]
     u = torch.from_numpy(ref_to_dev(u_ref, nd)).to(cuda)
     outs = {}
-    for v in range(6):
+    for v in range(7):
         try:
             solver.set_launch_variant(v)
         except Exception:
@@ -61,7 +61,7 @@ def test_node_shapes_every_degree(case, cuda):
         outs[v] = du
     assert 0 in outs and 3 in outs and 4 in outs, sorted(outs)
     node = outs[3].cpu().numpy()
-    for v in (0, 1, 2, 4, 5):
+    for v in (0, 1, 2, 4, 5, 6):
         if v in outs:
             assert rel_linf(node, outs[v].cpu().numpy()) <= RTOL, v
     ref = do.rhs(s, u_ref, 0.0)

@@ -290,7 +290,7 @@ def test_conservation_and_free_stream_large(cuda):
     assert float(du.abs().max()) <= 1e-10 * float(fs.abs().max()) / h
 
 
-@pytest.mark.parametrize("name", ["kh", "kh_hg", "dmr", "tgv", "ns", "vortex_n6"])
+@pytest.mark.parametrize("name", ["kh", "kh_hg", "dmr", "tgv", "tgv_partial", "ns", "vortex_n6"])
 def test_launch_variants(name, cuda):
     """The line-parallel launch shapes give the same bits, the node-parallel
     shape agrees to rounding and with the oracle, and the autotuner leaves
@@ -336,7 +336,21 @@ def test_launch_variants(name, cuda):
     if not pipe_variant:
         with pytest.raises(Exception):
             solver.set_launch_variant(5)
-    nvar = 6 if pipe_variant else 5 if node_variant else 3
+    # two nodes per thread (3D, n = 2 or 4, split form): the same fluxes, z
+    # pairs shared between threads (another summation order)
+    node2_variant = pipe_variant and nd == 3 and case["polydeg"] in (1, 3)
+    if node2_variant:
+        solver.set_launch_variant(6)
+        du6 = torch.empty_like(u)
+        solver.rhs(u, du6, 0.05)
+        torch.cuda.synchronize()
+        a = du6.cpu().numpy()
+        assert rel_linf(a, outs[0].cpu().numpy()) <= RTOL
+        assert rel_linf(dev_to_ref(a, solver.mesh.n_cells), do.rhs(s, u_ref, 0.05)) <= RTOL
+    else:
+        with pytest.raises(Exception):
+            solver.set_launch_variant(6)
+    nvar = 7 if node2_variant else 6 if pipe_variant else 5 if node_variant else 3
     chosen, times = solver.autotune(u, retime=True)
     torch.cuda.synchronize()
     assert chosen in range(nvar)

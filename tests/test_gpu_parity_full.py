@@ -110,7 +110,7 @@ def test_tgv16_kennedy_gruber_every_shape_matches_reference(cuda):
     solver = _solver(3, 3, cells, left, right, "kennedy_gruber", "llf")
     ud = torch.from_numpy(ref_to_dev(u0, 3)).to(cuda)
     du_r, bar = _bar(rc, u0, 0.0)
-    nshapes = 6
+    nshapes = 7  # 0-2 line, 3-4 node, 5 pipelined, 6 two nodes per thread
     for v in range(nshapes):
         solver.set_launch_variant(v)
         err = rel_linf(_rhs(solver, ud, 0.0), du_r)
@@ -255,7 +255,7 @@ def test_other_fluxes_3d_match_reference(vf, cuda):
     du_r, bar = _bar(rc, u, 0.0)
     solver = _solver(3, 3, c["cells"], c["left"], c["right"], vf, "llf")
     ud = torch.from_numpy(ref_to_dev(u, 3)).to(cuda)
-    for v in range(6):
+    for v in range(7):
         solver.set_launch_variant(v)
         err = rel_linf(_rhs(solver, ud, 0.0), du_r)
         assert err <= bar, (v, err, bar)

@@ -92,6 +92,45 @@ def test_static_scratch_step_allocates_nothing(cuda):
     assert free1 == free0
 
 
+class _DeviceView:
+    """A float64 vector at a raw device address (CUDA array interface)."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8",
+                                         "data": (ptr, False), "version": 3}
+
+
+def test_static_scratch_holds_the_stage_states(cuda):
+    """The stage states went to the static scratch (not to the context's
+    temporaries): after a step, its two slots hold u^(1) and u^(2) bit for bit
+    as dgsem_ssprk3_stage computes them into caller buffers."""
+    import torch
+
+    from dgsem_b200 import _capi as C
+    L = C.lib()
+    solver, sol, dt = _case("tgv")
+    u0 = sol.u.clone()
+    n = u0.numel()
+    s1 = torch.empty_like(u0)
+    s2 = torch.empty_like(u0)
+    C.check(L.dgsem_ssprk3_stage(solver.handle, 1, None, ctypes.c_void_p(u0.data_ptr()),
+                                 ctypes.c_void_p(s1.data_ptr()), 0.0, dt), "stage 1")
+    C.check(L.dgsem_ssprk3_stage(solver.handle, 2, ctypes.c_void_p(u0.data_ptr()),
+                                 ctypes.c_void_p(s1.data_ptr()),
+                                 ctypes.c_void_p(s2.data_ptr()), 0.0, dt), "stage 2")
+    u = u0.clone()
+    C.check(L.dgsem_ssprk3_step_static_scratch(solver.handle, ctypes.c_void_p(u.data_ptr()),
+                                               0.0, dt), "static-scratch step")
+    torch.cuda.synchronize()
+    for k, want in ((0, s1), (1, s2)):
+        ptr = ctypes.c_void_p()
+        C.check(L.dgsem_static_scratch_state(k, ctypes.byref(ptr)), "scratch state")
+        got = torch.as_tensor(_DeviceView(ptr.value, n), device=cuda)
+        assert torch.equal(got, want.reshape(-1)), k
+    bad = ctypes.c_void_p()
+    assert L.dgsem_static_scratch_state(2, ctypes.byref(bad)) == C.DGSEM_ERR_INVALID_ARG
+
+
 def test_static_scratch_rejects_large_state(cuda):
     import torch
 
