@@ -11,22 +11,24 @@
 namespace dgsem {
 namespace {
 
-// basis_detail.hpp:34-50
+// basis_detail.hpp:34-50: Legendre recurrence for P_n and its derivative up
+// to n = polydeg; q = (2n+1)/(n+1) (x P_n - P_{n-2}) and q' = (2n+1) P_n
+// (same operations and order as the reference, for bitwise equal nodes).
 void q_and_l(int polydeg, double x, double* q, double* qder, double* LN) {
-  double L_Nm2 = 1.0, L_Nm1 = x, Lder_Nm2 = 0.0, Lder_Nm1 = 1.0;
-  double L_N = 0.0, Lder_N = 0.0;
+  double p_prev2 = 1.0, p_prev = x, dp_prev2 = 0.0, dp_prev = 1.0;
+  double p_cur = 0.0, dp_cur = 0.0;
   for (int i = 2; i <= polydeg; ++i) {
-    L_N = ((double)(2.0 * i - 1.0) * x * L_Nm1 - (double)(i - 1.0) * L_Nm2) /
-          (double)i;
-    Lder_N = Lder_Nm2 + (double)(2.0 * i - 1.0) * L_Nm1;
-    L_Nm2 = L_Nm1;
-    L_Nm1 = L_N;
-    Lder_Nm2 = Lder_Nm1;
-    Lder_Nm1 = Lder_N;
+    p_cur = ((double)(2.0 * i - 1.0) * x * p_prev - (double)(i - 1.0) * p_prev2) /
+            (double)i;
+    dp_cur = dp_prev2 + (double)(2.0 * i - 1.0) * p_prev;
+    p_prev2 = p_prev;
+    p_prev = p_cur;
+    dp_prev2 = dp_prev;
+    dp_prev = dp_cur;
   }
-  *q = (double)(2.0 * polydeg + 1.0) / (polydeg + 1.0) * (x * L_N - L_Nm2);
-  *qder = (2.0 * polydeg + 1.0) * L_N;
-  *LN = L_N;
+  *q = (double)(2.0 * polydeg + 1.0) / (polydeg + 1.0) * (x * p_cur - p_prev2);
+  *qder = (2.0 * polydeg + 1.0) * p_cur;
+  *LN = p_cur;
 }
 
 void barycentric(int n, const double* nodes, double* wb) {
@@ -39,43 +41,47 @@ void barycentric(int n, const double* nodes, double* wb) {
   for (int i = 0; i < n; ++i) wb[i] = 1.0 / wb[i];
 }
 
+// Lagrange basis values at x divided by the weights (the lifting vector):
+// barycentric form, exact 1 at a node.
 void lhat(int n, double x, const double* nodes, const double* w, double* out) {
   double wb[kMaxNodes];
   barycentric(n, nodes, wb);
-  double poly[kMaxNodes] = {0};
-  bool hit = false;
+  double lag[kMaxNodes] = {0};
+  bool at_node = false;
   for (int i = 0; i < n; ++i) {
     if (std::abs(x - nodes[i]) < std::numeric_limits<double>::epsilon()) {
-      poly[i] = 1.0;
-      hit = true;
+      lag[i] = 1.0;
+      at_node = true;
       break;
     }
   }
-  if (!hit) {
-    for (int i = 0; i < n; ++i) poly[i] = wb[i] / (x - nodes[i]);
-    double total = 0.0;
-    for (int i = 0; i < n; ++i) total += poly[i];
-    for (int i = 0; i < n; ++i) poly[i] /= total;
+  if (!at_node) {
+    for (int i = 0; i < n; ++i) lag[i] = wb[i] / (x - nodes[i]);
+    double denom = 0.0;
+    for (int i = 0; i < n; ++i) denom += lag[i];
+    for (int i = 0; i < n; ++i) lag[i] /= denom;
   }
-  for (int i = 0; i < n; ++i) out[i] = poly[i] / w[i];
+  for (int i = 0; i < n; ++i) out[i] = lag[i] / w[i];
 }
 
+// Normalised Legendre polynomial sqrt(n + 1/2) P_n(x) (the modal basis of the
+// shock indicator's Vandermonde matrix).
 double legendre(int nn, double x) {
-  double poly = 0.0;
+  double p_n = 0.0;
   if (nn == 0) {
-    poly = 1.0;
+    p_n = 1.0;
   } else if (nn == 1) {
-    poly = x;
+    p_n = x;
   } else {
-    double p2 = 1.0, p1 = x;
+    double p_prev2 = 1.0, p_prev = x;
     for (int i = 2; i <= nn; ++i) {
-      poly = ((double)(2.0 * i - 1.0) * x * p1 - (double)(i - 1.0) * p2) /
-             (double)i;
-      p2 = p1;
-      p1 = poly;
+      p_n = ((double)(2.0 * i - 1.0) * x * p_prev - (double)(i - 1.0) * p_prev2) /
+            (double)i;
+      p_prev2 = p_prev;
+      p_prev = p_n;
     }
   }
-  return poly * std::sqrt(nn + 0.5);
+  return p_n * std::sqrt(nn + 0.5);
 }
 
 // base/container_fixed.hpp:117-162 (partial-pivot Gauss-Jordan)
