@@ -308,11 +308,76 @@ def reference_rate(workload: str, warmup: int, steps: int):
     return dofs * 3 * n / el, n, el, threads, nwarm
 
 
+def reference_rate_batched(warmup: int, steps: int):
+    """The reference's own path for the batched workload: one solver per mesh,
+    advanced mesh after mesh (the reference has no batched mode), on a bounded
+    sample of the 256 meshes (every 16th, 16 meshes over all degrees), each
+    with its own vortex and time step.  Returns (DOF-updates/s, sampled
+    meshes, timed steps per mesh, seconds, threads)."""
+    from oracle import dgsem_oracle as do
+    from oracle import ref_binding as rb
+    specs = batched_meshes()[::16]
+    left, right = (-5.0, -5.0), (5.0, 5.0)
+    cases = []
+    for cells, N, beta, centre in specs:
+        rc = rb.RefCase(rb.EULER2D_PERIODIC_SPLIT, N, cells, left, right,
+                        volume_flux=VF_CODE["chandrashekar"], surface_flux=SF_CODE["llf"])
+        s = do.Scheme(ndims=2, polydeg=N, cells=cells, left=left, right=right)
+        u = do.initial_state(s, "vortex", beta=beta, center=centre)
+        dt = 0.5 * (10.0 / cells[0]) / ((2.0 * (N + 1) - 1.0) * 4.0)
+        cases.append([rc, u, dt, cells[0] * cells[1] * (N + 1) ** 2])
+    for c in cases:  # warm-up
+        c[1] = c[0].ssprk3(c[1], 0.0, c[2], max(1, min(warmup, 2)))
+    # steps per mesh so that the sample takes CPU_MIN_SAMPLE_S .. CPU_MAX_SAMPLE_S
+    t0 = time.perf_counter()
+    for c in cases:
+        c[1] = c[0].ssprk3(c[1], 0.0, c[2], 1)
+    one = time.perf_counter() - t0
+    n = max(steps, math.ceil(CPU_MIN_SAMPLE_S / max(one, 1e-6)))
+    n = max(1, min(n, int(CPU_MAX_SAMPLE_S / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    for c in cases:
+        c[1] = c[0].ssprk3(c[1], 0.0, c[2], n)
+    el = time.perf_counter() - t0
+    dofs = sum(c[3] for c in cases)
+    return dofs * 3 * n / el, len(cases), n, el, rb.lib().dgsem_ref_omp_threads()
+
+
 def cpu_sample_text(workload: str, n: int, el: float, nwarm: int) -> str:
     return (f"{nwarm} warm-up + {n} timed SSPRK3 steps of the full {workload} mesh "
             f"({el:.1f} s; at least {CPU_MIN_SAMPLE_S:.0f} s, at most {CPU_MAX_SAMPLE_S:.0f} s "
             f"of timed CPU work); reference src/ compiled with the project's Kokkos shim, "
             f"OpenMP on all host threads; CPU: {cpu_model()}")
+
+
+def run_reference_batched(args):
+    """Reference arm of the batched workload (reference_rate_batched)."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    try:
+        rate, nmesh, n, el, threads = reference_rate_batched(args.warmup, args.steps)
+    except Exception as exc:  # reference library missing on this machine
+        print(json.dumps({"impl": "reference", "unavailable": f"{type(exc).__name__}: {exc}"}))
+        return 0
+    sample = (f"{nmesh} of the 256 meshes (every 16th, degrees 2-7), one reference solver "
+              f"each, {n} timed SSPRK3 steps per mesh after warm-up ({el:.1f} s); the "
+              f"reference has no batched mode, so its path is mesh after mesh; reference "
+              f"src/ compiled with the project's Kokkos shim, OpenMP on all host threads; "
+              f"CPU: {cpu_model()}")
+    line = {
+        "metric": "FP64 DOF-updates/s per RHS (batched)", "value": rate,
+        "unit": "DOF-updates/s", "impl": "reference", "n_gpus": args.gpus, "steps": n,
+        "warmup": args.warmup, "ms_per_step": 1e3 * el / n, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded isentropic vortices)",
+        "config": batched_config(),
+        "cpu_baseline": {"value": rate, "unit": "DOF-updates/s", "cores": threads,
+                         "kind": "reference", "sample": sample, "cpu_model": cpu_model()},
+        "e2e": {"value": rate, "unit": "DOF-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
 
 
 def run_reference_arm(args):
@@ -666,6 +731,18 @@ def batched_meshes(seed: int = 20260512, count: int = 256):
     return out
 
 
+def batched_config() -> dict:
+    """The batched workload's config, identical in both arms."""
+    specs = batched_meshes()
+    dofs = sum(cells[0] * cells[1] * (N + 1) ** 2 for cells, N, _, _ in specs)
+    return {"workload": "batched", "meshes": len(specs), "dofs": dofs,
+            "degrees": sorted({N for _, N, _, _ in specs}),
+            "volume_flux": "chandrashekar", "surface_flux": "llf",
+            "l2": "inputs larger than L2 (state %.2f GB)" % (dofs * 32 / 1e9),
+            "graph": "one SSPRK3 step per graph replay (per-degree launches as parallel "
+                     "branches, or one persistent launch per stage)"}
+
+
 def run_batched(args):
     """Batched multi-mesh throughput and speedup over the per-instance path."""
     print(json.dumps(measure_batched(args)))
@@ -768,12 +845,8 @@ def measure_batched(args):
         "unit": "DOF-updates/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": batched_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded isentropic vortices)",
-        "config": {"workload": "batched", "meshes": len(specs), "dofs": dofs,
-                   "degrees": sorted({N for _, N, _, _ in specs}),
-                   "volume_flux": "chandrashekar", "surface_flux": "llf",
-                   "l2": "inputs larger than L2 (state %.2f GB)" % (dofs * 32 / 1e9),
-                   "graph": "one SSPRK3 step per graph replay (per-degree launches as parallel branches, or one persistent launch per stage)",
-                   "launch_variants": variants},
+        "config": batched_config(),
+        "launch_variants": variants,
         "speedup_vs_per_instance": plain_ms / batched_ms,
         "launch_mode": mode,
         "ms_per_step_by_mode": mode_ms,
@@ -953,9 +1026,7 @@ def main():
         args.steps = DEFAULT_STEPS[args.workload]
     if args.workload == "batched":
         if args.impl == "reference":
-            print(json.dumps({"impl": "reference", "unavailable":
-                              "the reference has no batched multi-mesh mode"}))
-            return 0
+            return run_reference_batched(args)
         return run_batched(args)
     if args.workload == "adjoint":
         if args.impl == "reference":

@@ -7,7 +7,8 @@ ABI in include/dgsem_b200.h); this package is its host-side mirror.
 from ._capi import DgsemError, lib  # noqa: F401
 from .solver import (  # noqa: F401
     BoundarySet, ChandrashekarFlux, CompressibleEuler2D, CompressibleEuler3D,
-    CompressibleNavierStokes2D, DirichletBC, DoubleMachReflectionInitial, HGIndicator,
+    CompressibleNavierStokes2D, CompressibleNavierStokes3D, DirichletBC,
+    DoubleMachReflectionInitial, HGIndicator,
     HLLCFlux, InviscidTaylorGreenVortex, IsentropicVortex, KelvinHelmholtzInitial,
     KennedyGruberFlux, LaxFriedrichsFlux, LobattoLegendreBasis,
     MixedDirichletSlipWallBC, NSNoSlipAdiabaticWallBC, NSSlipAdiabaticWallBC, OutflowBC,

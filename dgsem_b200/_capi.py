@@ -23,7 +23,7 @@ DGSEM_ERR_SCRATCH_LIMIT = 7
 STATIC_SCRATCH_MAX_STATE = 2097152  # DGSEM_STATIC_SCRATCH_MAX_STATE (doubles per stage state)
 
 # enums (include/dgsem_b200.h)
-EULER_2D, EULER_3D, NAVIER_STOKES_2D = 0, 1, 2
+EULER_2D, EULER_3D, NAVIER_STOKES_2D, NAVIER_STOKES_3D = 0, 1, 2, 3
 VF_CHANDRASHEKAR, VF_RANOCHA, VF_KENNEDY_GRUBER = 0, 1, 2
 SF_LAX_FRIEDRICHS, SF_HLLC = 0, 1
 VI_SPLIT_FORM, VI_SHOCK_CAPTURING_HG = 0, 1

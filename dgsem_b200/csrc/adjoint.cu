@@ -75,7 +75,7 @@ class AdjointEngine final : public AdjointEngineBase {
     fill_basis_const<N>(cfg.basis, &a.basis);
     const unsigned blocks = (unsigned)((cfg.nelem + EPB - 1) / EPB);
     if constexpr (NS) {
-      GradArgs<N> ga;
+      GradArgs<N> ga{};
       ga.u = u;
       ga.grad = cfg.grad;
       for (int i = 0; i < 3; ++i) ga.cells[i] = cfg.cells[i];

@@ -162,6 +162,10 @@ __global__ void layout_kernel(const double* src, double* dst, int ndims,
   }
 }
 
+bool is_navier_stokes(int equation) {
+  return equation == DGSEM_NAVIER_STOKES_2D || equation == DGSEM_NAVIER_STOKES_3D;
+}
+
 dgsem_status validate(const dgsem_mesh_desc* m, const dgsem_scheme_desc* s) {
   if (!m || !s) return DGSEM_ERR_INVALID_ARG;
   if (m->ndims != 2 && m->ndims != 3) return DGSEM_ERR_INVALID_ARG;
@@ -170,8 +174,10 @@ dgsem_status validate(const dgsem_mesh_desc* m, const dgsem_scheme_desc* s) {
     if (m->n_cells[a] < 1 || m->n_cells[a] > (int64_t)1 << 24) return DGSEM_ERR_INVALID_ARG;
     if (!(m->domain_right[a] > m->domain_left[a])) return DGSEM_ERR_INVALID_ARG;
   }
-  const int want_dims = s->equation == DGSEM_EULER_3D ? 3 : 2;
-  if (s->equation < 0 || s->equation > 2) return DGSEM_ERR_INVALID_ARG;
+  const bool ns = s->equation == DGSEM_NAVIER_STOKES_2D || s->equation == DGSEM_NAVIER_STOKES_3D;
+  const int want_dims =
+      s->equation == DGSEM_EULER_3D || s->equation == DGSEM_NAVIER_STOKES_3D ? 3 : 2;
+  if (s->equation < 0 || s->equation > 3) return DGSEM_ERR_INVALID_ARG;
   if (want_dims != m->ndims) return DGSEM_ERR_INVALID_ARG;
   if (s->volume_flux < 0 || s->volume_flux > 2) return DGSEM_ERR_INVALID_ARG;
   if (s->surface_flux < 0 || s->surface_flux > 1) return DGSEM_ERR_INVALID_ARG;
@@ -194,10 +200,11 @@ dgsem_status validate(const dgsem_mesh_desc* m, const dgsem_scheme_desc* s) {
   if (s->volume_integral == DGSEM_VI_SHOCK_CAPTURING_HG) {
     if (!(s->alpha_min >= 0.0 && s->alpha_max >= 0.0)) return DGSEM_ERR_INVALID_ARG;
   }
-  if (s->equation == DGSEM_NAVIER_STOKES_2D) {
+  if (ns) {
     if (s->volume_integral != DGSEM_VI_SPLIT_FORM) return DGSEM_ERR_UNSUPPORTED;
-    // periodic directions or the Navier-Stokes adiabatic walls
-    for (int f = 0; f < 4; ++f)
+    // periodic directions or (2D) the Navier-Stokes adiabatic walls; 3D
+    // meshes are periodic (checked above)
+    for (int f = 0; f < 2 * m->ndims; ++f)
       if (s->bc[f] != DGSEM_BC_PERIODIC && s->bc[f] != DGSEM_BC_NS_NOSLIP_ADIABATIC_WALL &&
           s->bc[f] != DGSEM_BC_NS_SLIP_ADIABATIC_WALL)
         return DGSEM_ERR_UNSUPPORTED;
@@ -266,7 +273,7 @@ dgsem_status dgsem_ctx_create(const dgsem_mesh_desc* mesh,
   std::unique_ptr<EngineBase> engine;
   try {
     engine = make_engine(nd, n, scheme->volume_flux, scheme->surface_flux, hg,
-                         scheme->equation == DGSEM_NAVIER_STOKES_2D);
+                         is_navier_stokes(scheme->equation));
   } catch (...) {
     return DGSEM_ERR_ALLOC;
   }
@@ -369,8 +376,9 @@ dgsem_status dgsem_ctx_create(const dgsem_mesh_desc* mesh,
   ctx->tdev = ctx->staging ? device_alloc<double>(ctx, 1, &err) : nullptr;
   ctx->flag = ctx->tdev ? device_alloc<unsigned int>(ctx, 1, &err) : nullptr;
   c.grad = nullptr;
-  if (ctx->flag && scheme->equation == DGSEM_NAVIER_STOKES_2D) {
-    c.grad = device_alloc<double>(ctx, (size_t)c.nelem * 8 * ctx->nodes, &err);
+  if (ctx->flag && is_navier_stokes(scheme->equation)) {
+    // four gradient variables x ndims directions per node
+    c.grad = device_alloc<double>(ctx, (size_t)c.nelem * 4 * nd * ctx->nodes, &err);
     if (!c.grad) ctx->flag = nullptr;
   }
   if (!ctx->flag) {
@@ -575,7 +583,7 @@ dgsem_status dgsem_graph_destroy(dgsem_graph* g) {
 dgsem_status dgsem_indicator(dgsem_ctx* ctx, const double* u, double* alpha,
                              uint8_t* flags) {
   if (!ctx || !u) return DGSEM_ERR_INVALID_ARG;
-  if (ctx->scheme.equation == DGSEM_NAVIER_STOKES_2D) return DGSEM_ERR_UNSUPPORTED;
+  if (is_navier_stokes(ctx->scheme.equation)) return DGSEM_ERR_UNSUPPORTED;
   const EngineConfig& c = ctx->cfg;
   const int threads = 128;
   const unsigned blocks = (unsigned)((c.nelem + threads - 1) / threads);
@@ -870,7 +878,7 @@ dgsem_status dgsem_autotune(dgsem_ctx* ctx, const double* u, int* chosen, double
   const bool warm = std::getenv("DGSEM_AUTOTUNE_WARM") != nullptr;
   const std::string key =
       tune_key(c.ndims, c.n, ctx->scheme.volume_flux, ctx->scheme.surface_flux,
-               ctx->scheme.volume_integral, ctx->scheme.equation == DGSEM_NAVIER_STOKES_2D,
+               ctx->scheme.volume_integral, is_navier_stokes(ctx->scheme.equation),
                c.nelem) +
       (warm ? "_warm" : "_cold");
   std::lock_guard<std::mutex> lock(tune_mutex());

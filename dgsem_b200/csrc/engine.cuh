@@ -181,11 +181,12 @@ void launch_stage_kernel(void (*kernel)(P...), unsigned grid, unsigned block, si
 template <int DIM, int N, int VF, int SF, bool HG, bool NS = false>
 class Engine final : public EngineBase {
  public:
-  static constexpr int GRAD_EPB = (128 / (N * N)) > 0 ? (128 / (N * N)) : 1;
+  static constexpr int GRAD_EPB = (128 / ipow(N, DIM)) > 0 ? (128 / ipow(N, DIM)) : 1;
   static constexpr bool kBatch = !NS && !HG;
-  // the line-parallel shapes 0-2 carry shock capturing in 2D only; 3D shock
-  // capturing runs on the node-parallel shapes (0-2 then run shape 3)
-  static constexpr bool kLine = !(DIM == 3 && HG);
+  // the line-parallel shapes 0-2 carry shock capturing and the viscous terms
+  // in 2D only; in 3D these run on the node-parallel shapes (0-2 then run
+  // shape 3)
+  static constexpr bool kLine = !(DIM == 3 && (HG || NS));
 
   template <int V>
   using Sh = StageShape<DIM, N, VF, SF, HG, LaunchShape<DIM, N, V>::EPB, NS>;
@@ -357,7 +358,7 @@ class Engine final : public EngineBase {
     args.mesh.nelem = (int)cfg.nelem;
     args.mesh.tab = cfg.tab;
     if constexpr (NS) {
-      GradArgs<N> ga;
+      GradArgs<N> ga{};
       ga.u = u_in;
       ga.grad = cfg.grad;
       for (int i = 0; i < 3; ++i) ga.cells[i] = cfg.cells[i];
@@ -365,11 +366,15 @@ class Engine final : public EngineBase {
       ga.gamma = cfg.gamma;
       ga.tab = cfg.tab;
       ga.basis = args.basis;
-      for (int d = 0; d < 2; ++d) ga.periodic[d] = cfg.periodic[d];
-      for (int f = 0; f < 4; ++f) ga.bc_kind[f] = cfg.bc.kind[f];
+      for (int d = 0; d < DIM; ++d) ga.periodic[d] = cfg.periodic[d];
+      for (int f = 0; f < 2 * DIM; ++f) ga.bc_kind[f] = cfg.bc.kind[f];
       const int64_t gblocks = (cfg.nelem + GRAD_EPB - 1) / GRAD_EPB;
-      launch_stage_kernel(br1_gradient_kernel<N, GRAD_EPB>, (unsigned)gblocks, GRAD_EPB * N * N, 0,
-                          s, ga);
+      if constexpr (DIM == 2)
+        launch_stage_kernel(br1_gradient_kernel<N, GRAD_EPB>, (unsigned)gblocks, GRAD_EPB * N * N,
+                            0, s, ga);
+      else
+        launch_stage_kernel(br1_gradient_kernel_3d<N, GRAD_EPB>, (unsigned)gblocks,
+                            GRAD_EPB * N * N * N, 0, s, ga);
     }
     switch (variant_) {
       case 1: launch<1>(args, cfg.nelem, s); break;

@@ -551,6 +551,11 @@ __device__ __forceinline__ void ns_gradient_variables(const double* u, double ga
 __device__ __forceinline__ void ns_neg_viscous_flux(const double* q, const double* gx,
                                                     const double* gy, double mu,
                                                     double kappa, int dim, double* f);
+__device__ __forceinline__ void ns_gradient_variables_3d(const double* u, double gamma,
+                                                         double* q);
+__device__ __forceinline__ void ns_neg_viscous_flux_3d(const double* q, const double (*g)[4],
+                                                       double mu, double kappa, int dim,
+                                                       double* f);
 
 // Element index over the axes != c of the element whose coordinate along
 // `dir` is replaced by `pos` (the neighbour across a face of direction dir).
@@ -635,7 +640,30 @@ __device__ __forceinline__ void element_face_flux_state(
   } else {
     surface_flux<DIM, SF>(sx, so, nrm, gamma, f);
   }
-  if constexpr (NS) {
+  if constexpr (NS && DIM == 3) {
+    // 3D periodic meshes: the one-sided viscous interface flux -F_v . n of the
+    // high-side (primary) element at its low-face node
+    // (parabolic_viscous.hpp:570-585), lifted like the inviscid flux
+    double w[3][5];
+    if (side) {
+      double q[5], g[3][4];
+      ns_gradient_variables_3d(ux, gamma, q);
+      const double* G = p.grad + (int64_t)en * 4 * 3 * ND + nb_node;
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) g[d][v] = __ldg(G + (v * 3 + d) * ND);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) ns_neg_viscous_flux_3d(q, g, p.mu, p.kappa, d, w[d]);
+    } else {
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int v = 0; v < 5; ++v) w[d][v] = wv_el[(d * NV + v) * NDP + opn];
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) f[v] += w[0][v] * nrm[0] + w[1][v] * nrm[1] + w[2][v] * nrm[2];
+  } else if constexpr (NS) {
     if (en >= 0) {
       // one-sided viscous interface flux: -F_v . n of the high-side (primary)
       // element at its low-face node (parabolic_viscous.hpp:570-585), lifted

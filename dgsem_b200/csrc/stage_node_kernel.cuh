@@ -87,8 +87,8 @@ struct NodeShape {
   // smem_bytes_base and leave the rest of the SM's storage to L1
   static constexpr int SM_N = (NV * ND) % 2 == 0 ? EPB * NV * ND : 0;
   static constexpr int NT = EPB * ND;
-  // Navier-Stokes: -F_v per node [el][dim][var][node] (2D)
-  static constexpr int SM_W = NS ? EPB * 2 * NV * ND : 0;
+  // Navier-Stokes: -F_v per node [el][dim][var][node]
+  static constexpr int SM_W = NS ? EPB * DIM * NV * ND : 0;
   static constexpr size_t smem_bytes_base =
       sizeof(double) * (SM_U + SM_P + SM_F + SM_A + SM_VINV + SM_X + SM_W) +
       sizeof(int) * EPB * NI;
@@ -432,12 +432,15 @@ __device__ __forceinline__ void node_lift(const double* sf_el, int node, double 
 
 // Phase 2a of the node-parallel kernels: the interface / boundary flux f* of
 // every (element, face, face node) of the tile, once, into the face buffer
-// sf[el][face][fn][var].  Tasks are grouped by (side, direction), both
-// compile-time constants in the flux code (no runtime-indexed arrays);
-// inside a group the order is element-major, and a group fills whole warps
-// where ne * NF is a multiple of 32, so a warp's lanes share the face side
-// and direction and evaluate the flux in one argument order.  Task idx of
-// the tile goes to thread idx % NT, as in one block-stride loop.
+// sf[el][face][fn][var].  The lanes of a warp share the face side, so they
+// evaluate the flux in one argument order.
+//   3D: tasks grouped by (side, direction), both compile-time constants in
+//       the flux code (no runtime-indexed arrays); inside a group the order
+//       is element-major, and a group fills whole warps where ne * NF is a
+//       multiple of 32.  Task idx of the tile goes to thread idx % NT.
+//   2D: one block-stride loop over the tasks in side-major order with the
+//       direction at run time (measured faster there: the boundary branch
+//       of the flux code then exists once).
 template <int DIM, int N, int VF, int SF, bool NS, int NDP, int NT, int NQ, int NI>
 __device__ __forceinline__ void node_face_tasks(const StageArgs<N>& p, const MeshView& M,
                                                 const double* us, const double* pr,
@@ -446,38 +449,46 @@ __device__ __forceinline__ void node_face_tasks(const StageArgs<N>& p, const Mes
                                                 int c0, int c1, int c2) {
   using K = NodeKernelSlots<DIM, VF>;
   constexpr int NV = DIM + 2, ND = ipow(N, DIM), NF = ipow(N, DIM - 1), NFACE = 2 * DIM;
-  const int gsz = ne * NF;
+  auto task = [&](int side, int dir, int fe, int fn) {
+    const int face = 2 * dir + side;
+    const int* I = info + fe * NI;
+    const double* U = us + fe * NV * NDP;
+    const double* P = pr + fe * NQ * NDP;
+    const int opn = padn<N, NDP != ND>(line_node<DIM, N>(dir, fn, side ? N - 1 : 0));
+    FaceState<DIM> so;
 #pragma unroll
-  for (int side = 0; side < 2; ++side) {
+    for (int q = 0; q < NV; ++q) so.u[q] = U[q * NDP + opn];
+    const double g = K::HALF ? 2.0 : 1.0;
 #pragma unroll
-    for (int dir = 0; dir < DIM; ++dir) {
-      const int gbase = (side * DIM + dir) * gsz;
-      int r = tid - gbase % NT;
-      if (r < 0) r += NT;
-      for (; r < gsz; r += NT) {
-        const int fe = r / NF, fn = r - (r / NF) * NF;
-        const int face = 2 * dir + side;
-        const int* I = info + fe * NI;
-        const double* U = us + fe * NV * NDP;
-        const double* P = pr + fe * NQ * NDP;
-        const int opn = padn<N, NDP != ND>(line_node<DIM, N>(dir, fn, side ? N - 1 : 0));
-        FaceState<DIM> so;
+    for (int d = 0; d < DIM; ++d) so.v[d] = g * P[(K::V + d) * NDP + opn];
+    so.p = g * P[K::P * NDP + opn];
+    so.a2 = P[K::A * NDP + opn];
+    double f[NV];
+    element_face_flux_state<DIM, N, VF, SF, NS, NDP>(p, M, so, U,
+                                                     NS ? wv + fe * DIM * NV * ND : nullptr, I,
+                                                     dir, side, fn, gamma, t_stage, c0, c1, c2,
+                                                     f);
+    double* F = sf + ((fe * NFACE + face) * NF + fn) * NV;
 #pragma unroll
-        for (int q = 0; q < NV; ++q) so.u[q] = U[q * NDP + opn];
-        const double g = K::HALF ? 2.0 : 1.0;
+    for (int q = 0; q < NV; ++q) F[q] = f[q];
+  };
+  if constexpr (DIM == 3) {
+    const int gsz = ne * NF;
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) so.v[d] = g * P[(K::V + d) * NDP + opn];
-        so.p = g * P[K::P * NDP + opn];
-        so.a2 = P[K::A * NDP + opn];
-        double f[NV];
-        element_face_flux_state<DIM, N, VF, SF, NS, NDP>(p, M, so, U,
-                                                         NS ? wv + fe * 2 * NV * ND : nullptr,
-                                                         I, dir, side, fn, gamma, t_stage, c0,
-                                                         c1, c2, f);
-        double* F = sf + ((fe * NFACE + face) * NF + fn) * NV;
+    for (int side = 0; side < 2; ++side) {
 #pragma unroll
-        for (int q = 0; q < NV; ++q) F[q] = f[q];
+      for (int dir = 0; dir < DIM; ++dir) {
+        const int gbase = (side * DIM + dir) * gsz;
+        int r = tid - gbase % NT;
+        if (r < 0) r += NT;
+        for (; r < gsz; r += NT) task(side, dir, r / NF, r - (r / NF) * NF);
       }
+    }
+  } else {
+    for (int idx = tid; idx < ne * NFACE * NF; idx += NT) {
+      const int side = idx >= ne * DIM * NF ? 1 : 0;
+      const int r = idx - side * ne * DIM * NF;
+      task(side, (r / NF) % DIM, r / (DIM * NF), r % NF);
     }
   }
 }
@@ -485,7 +496,7 @@ __device__ __forceinline__ void node_face_tasks(const StageArgs<N>& p, const Mes
 template <int DIM, int N, int VF, int SF, int EPB, bool BATCH, bool HG, bool NS = false,
           int NTB = 0, bool PERSIST = false>
 __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile = 0) {
-  static_assert(!NS || (DIM == 2 && !HG && !BATCH), "Navier-Stokes: 2D split form");
+  static_assert(!NS || (!HG && !BATCH), "Navier-Stokes: split form, single mesh");
   using S = NodeShape<DIM, N, VF, EPB, HG, NS>;
   using K = NodeKernelSlots<DIM, VF>;
   constexpr int NV = S::NV, ND = S::ND, NDP = S::NDP, NF = S::NF, NFACE = S::NFACE,
@@ -556,7 +567,23 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile 
 #pragma unroll
     for (int q = 0; q < NV; ++q) u[q] = us[(el * NV + q) * NDP + pn];
     node_prepare<DIM, N, VF, NDP>(M, u, gamma, info + el * NI, node, pr + el * NQ * NDP + pn);
-    if constexpr (NS) {
+    if constexpr (NS && DIM == 3) {
+      // -F_v at the node from the lifted gradient (parabolic_viscous.hpp:358-396)
+      double q[5], g[3][4];
+      ns_gradient_variables_3d(u, gamma, q);
+      const double* G = p.grad + (int64_t)(e0 + el) * 4 * 3 * ND + node;
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) g[d][v] = __ldg(G + (v * 3 + d) * ND);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double f[5];
+        ns_neg_viscous_flux_3d(q, g, p.mu, p.kappa, d, f);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) wv[((el * 3 + d) * NV + v) * ND + node] = f[v];
+      }
+    } else if constexpr (NS) {
       // -F_v at the node from the lifted gradient (parabolic_viscous.hpp:358-396)
       double q[4], gx[4], gy[4];
       ns_gradient_variables(u, gamma, q);
@@ -672,7 +699,29 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile 
       node_volume_direction<2, DIM, N, VF, NDP, WARP_ALL, S::XCHG>(p, M, U, P, I, node, pn, own,
                                                                   hgm1, acc, xbuf, tid, NT,
                                                                   worker);
-    if constexpr (NS) {
+    if constexpr (NS && DIM == 3) {
+      // viscous weak-form volume term sum_k Dhat(m, k) Ja^dir(k) . (-F_v)(k)
+      // along each line through the node (parabolic_viscous.hpp:398-469)
+      const double* W = wv + ev * 3 * NV * ND;
+#pragma unroll
+      for (int dir = 0; dir < 3; ++dir) {
+        const int m = dir == 0 ? node % N : dir == 1 ? (node / N) % N : node / (N * N);
+        const int stride = dir == 0 ? 1 : dir == 1 ? N : N * N;
+        const double* j0 = M.tab.ja[dir][0] + (int64_t)I[3] * ND;
+        const double* j1 = M.tab.ja[dir][1] + (int64_t)I[4] * ND;
+        const double* j2 = M.tab.ja[dir][2] + (int64_t)I[5] * ND;
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+          const int nk = node + (k - m) * stride;
+          const double a0 = __ldg(j0 + nk), a1 = __ldg(j1 + nk), a2 = __ldg(j2 + nk);
+          const double dmk = p.basis.Dhat[m][k];
+#pragma unroll
+          for (int q = 0; q < NV; ++q)
+            acc[q] += dmk * (a0 * W[(0 * NV + q) * ND + nk] + a1 * W[(1 * NV + q) * ND + nk] +
+                             a2 * W[(2 * NV + q) * ND + nk]);
+        }
+      }
+    } else if constexpr (NS) {
       // viscous weak-form volume term sum_k Dhat(m, k) Ja^dir(k) . (-F_v)(k)
       // along each line through the node (parabolic_viscous.hpp:418-466)
       const double* W = wv + ev * 2 * NV * ND;

@@ -40,8 +40,11 @@ def combos():
 
 
 def ns_combos():
-    # 2D Navier-Stokes (BR1, periodic): n in 2..8, the three volume fluxes, LLF.
-    return sorted((2, n, vf, 0, 0, 1) for n in range(2, 9) for vf in range(3))
+    # 2D Navier-Stokes (BR1, periodic or walls): n in 2..8, the three volume
+    # fluxes, LLF; 3D Navier-Stokes (periodic): n in 2..5, the three volume
+    # fluxes, LLF (node-parallel shapes).
+    return (sorted((2, n, vf, 0, 0, 1) for n in range(2, 9) for vf in range(3)) +
+            sorted((3, n, vf, 0, 0, 1) for n in range(2, 6) for vf in range(3)))
 
 
 def generate() -> list[str]:

@@ -3,7 +3,7 @@
 Names and argument meaning follow RetrO598/DGSEM:
   StructuredMesh(domain_left, domain_right, n_cells)   mesh/structured_mesh.hpp:10-71
   LobattoLegendreBasis(polydeg)                         polynomial_basis/basis.hpp:12-182
-  CompressibleEuler2D/3D, CompressibleNavierStokes2D    equations/*.hpp
+  CompressibleEuler2D/3D, CompressibleNavierStokes2D/3D equations/*.hpp
   ChandrashekarFlux, LaxFriedrichsFlux (+ RanochaFlux, KennedyGruberFlux, HLLCFlux)
   VolumeIntegralSplitForm, VolumeIntegralShockCapturingHG, HGIndicator
                                                         space_integral/volume_flux.hpp:686-879
@@ -83,6 +83,18 @@ class CompressibleNavierStokes2D:
     NDIMS = 2
     NVARS = 4
     code = C.NAVIER_STOKES_2D
+
+
+@dataclass(frozen=True)
+class CompressibleNavierStokes3D:
+    """equations/compressible_navier_stokes3D.hpp (periodic boxes: the
+    reference's 3D Navier-Stokes setups are periodic)."""
+    gamma: float = 1.4
+    mu: float = 6.25e-4
+    prandtl: float = 0.72
+    NDIMS = 3
+    NVARS = 5
+    code = C.NAVIER_STOKES_3D
 
 
 # ---------------------------------------------------------------- fluxes

@@ -56,7 +56,8 @@ typedef enum dgsem_status {
 typedef enum dgsem_equation {
   DGSEM_EULER_2D = 0,          /* equations/compressible_euler2D.hpp */
   DGSEM_EULER_3D = 1,          /* equations/compressible_euler3D.hpp */
-  DGSEM_NAVIER_STOKES_2D = 2   /* equations/compressible_navier_stokes2D.hpp */
+  DGSEM_NAVIER_STOKES_2D = 2,  /* equations/compressible_navier_stokes2D.hpp */
+  DGSEM_NAVIER_STOKES_3D = 3   /* equations/compressible_navier_stokes3D.hpp (periodic boxes) */
 } dgsem_equation;
 
 typedef enum dgsem_volume_flux {

@@ -33,6 +33,7 @@
 #include <cstring>
 #include <memory>
 #include <numbers>
+#include <type_traits>
 
 extern "C" {
 // Case kinds understood by the harness.
@@ -47,6 +48,7 @@ enum {
   REF_EULER2D_CURVED_CENTRAL = 7,     // curvilinear periodic mesh, CentralFlux + LLF
   REF_EULER3D_CURVED = 8,             // curvilinear periodic mesh, Chandrashekar + LLF
   REF_NS2D_CHANNEL_WALLS = 9,         // NS, x periodic, no-slip bottom / slip top walls
+  REF_NS3D_PERIODIC_SPLIT = 10,       // 3D Navier-Stokes BR1 + split form, periodic box
 };
 
 typedef struct {
@@ -344,6 +346,8 @@ class RefCase final : public RefCaseBase {
   }
 
   void alpha(const T* u, T* a) override {
+    // the reference defines no shock indicator for 3D Navier-Stokes
+    if constexpr (!std::is_same_v<Eq, DGSEM::equations::CompressibleNavierStokes3D<T>>) {
     std::memcpy(sol_.u_device.data(), u, state_size() * sizeof(T));
     using ElementArray =
         typename DGSEM::solution_type_traits<T, D>::ElementArray;
@@ -358,6 +362,7 @@ class RefCase final : public RefCaseBase {
                                       Basis::device_data());
     ind(cells, sol_.u_device, av);
     std::memcpy(a, av.data(), av.size() * sizeof(T));
+    }
   }
 
   void steps(T* u, T t0, T dt, int n) override {
@@ -518,6 +523,7 @@ RefCaseBase* make_case_n(const dgsem_ref_case& c) {
   using E2 = DGSEM::equations::CompressibleEuler2D<T>;
   using E3 = DGSEM::equations::CompressibleEuler3D<T>;
   using NS2 = DGSEM::equations::CompressibleNavierStokes2D<T>;
+  using NS3 = DGSEM::equations::CompressibleNavierStokes3D<T>;
   using P = DGSEM::PeriodicBC;
   switch (c.kind) {
     case REF_EULER2D_PERIODIC_SPLIT: {
@@ -611,14 +617,23 @@ RefCaseBase* make_case_n(const dgsem_ref_case& c) {
       return new RefCase<NS2, N, VF, decltype(b), 2>(
           c, NS2{c.gamma, c.mu, c.prandtl}, b, true);
     }
+    case REF_NS3D_PERIODIC_SPLIT: {
+      if constexpr (N <= 4) {
+        using VF = DGSEM::VolumeIntegralSplitForm<Basis, NS3, DGSEM::ChandrashekarFlux>;
+        auto b = DGSEM::BoundarySet(P{}, P{}, P{}, P{}, P{}, P{});
+        return new RefCase<NS3, N, VF, decltype(b), 3>(c, NS3{c.gamma, c.mu, c.prandtl}, b,
+                                                       true);
+      }
+      return nullptr;
+    }
     default:
       return nullptr;
   }
 }
 
 RefCaseBase* make_case(const dgsem_ref_case& c) {
-  const bool is3d = c.kind == REF_EULER3D_PERIODIC_SPLIT ||
-                    c.kind == REF_EULER3D_PERIODIC_HG || c.kind == REF_EULER3D_CURVED;
+  const bool is3d = c.kind == REF_EULER3D_PERIODIC_SPLIT || c.kind == REF_EULER3D_PERIODIC_HG ||
+                    c.kind == REF_EULER3D_CURVED || c.kind == REF_NS3D_PERIODIC_SPLIT;
   if (is3d) {
     switch (c.polydeg) {
       case 1: return make_case_n<1>(c);
