@@ -768,7 +768,11 @@ def measure_batched(args):
     batch = D.BatchSolver(eq, meshes, D.ChandrashekarFlux, D.LaxFriedrichsFlux)
     batch.initialize(C.IC_ISENTROPIC_VORTEX, [(b, c[0], c[1]) for _, _, b, c in specs])
     stream = batch.stream
-    variants = batch.autotune(dts) if args.variant == "auto" else None
+    if args.variant == "auto":
+        variants = batch.autotune(dts)
+    else:
+        batch.set_launch_variant(int(args.variant))
+        variants = [int(args.variant)] * len({N for _, N, _, _ in specs})
 
     def timed_graph(persistent: bool):
         """Graph-replayed steps in one launch mode: (step times, launches, clocks)."""

@@ -45,7 +45,8 @@ EXPORTED = [
     "dgsem_batch_initial_condition", "dgsem_batch_ssprk3_step", "dgsem_batch_graph_create",
     "dgsem_batch_graph_launch", "dgsem_batch_graph_destroy", "dgsem_batch_check_finite",
     "dgsem_batch_launch_count", "dgsem_autotune", "dgsem_set_launch_variant",
-    "dgsem_batch_autotune", "dgsem_ssprk3_step_static_scratch", "dgsem_static_scratch_state",
+    "dgsem_batch_autotune", "dgsem_batch_set_launch_variant", "dgsem_ssprk3_step_static_scratch",
+    "dgsem_static_scratch_state",
     "dgsem_adjoint_create", "dgsem_adjoint_destroy", "dgsem_adjoint_rhs_vjp",
     "dgsem_kinetic_energy", "dgsem_adjoint_gradient", "dgsem_coordinates_host",
     "dgsem_fp64_fma_peak", "dgsem_write_vtu", "dgsem_write_vtu_host",
@@ -131,6 +132,7 @@ def lib() -> ctypes.CDLL:
     L.dgsem_autotune.argtypes = [vp, dp, c.POINTER(c.c_int), c.POINTER(c.c_double)]
     L.dgsem_set_launch_variant.argtypes = [vp, c.c_int]
     L.dgsem_batch_autotune.argtypes = [vp, dp, c.POINTER(c.c_double), c.POINTER(c.c_int)]
+    L.dgsem_batch_set_launch_variant.argtypes = [vp, c.c_int]
     L.dgsem_ssprk3_step_static_scratch.argtypes = [vp, dp, c.c_double, c.c_double]
     L.dgsem_static_scratch_state.argtypes = [c.c_int, c.POINTER(c.c_void_p)]
     L.dgsem_adjoint_create.argtypes = [vp, c.c_int, c.c_int, c.POINTER(vp)]

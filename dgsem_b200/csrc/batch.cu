@@ -296,6 +296,17 @@ dgsem_status dgsem_batch_autotune(dgsem_batch* b, double* u, const double* dt_ho
   return st;
 }
 
+dgsem_status dgsem_batch_set_launch_variant(dgsem_batch* b, int variant) {
+  if (!b) return DGSEM_ERR_INVALID_ARG;
+  for (const Group& g : b->groups)
+    if (variant < 0 || variant >= g.engine->num_variants()) return DGSEM_ERR_INVALID_ARG;
+  for (Group& g : b->groups) {
+    g.engine->set_variant(variant);
+    if (build_tiles(b, g) != cudaSuccess) return DGSEM_ERR_CUDA;
+  }
+  return DGSEM_OK;
+}
+
 dgsem_status dgsem_batch_create(const dgsem_mesh_desc* meshes, int n_meshes,
                                 const dgsem_scheme_desc* scheme, void* stream,
                                 dgsem_batch** out) {

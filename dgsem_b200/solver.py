@@ -633,6 +633,11 @@ class BatchSolver:
                                              chosen), "dgsem_batch_autotune")
         return list(chosen)
 
+    def set_launch_variant(self, variant: int) -> None:
+        """One launch shape for every degree group (dgsem_batch_set_launch_variant)."""
+        C.check(C.lib().dgsem_batch_set_launch_variant(self._h, int(variant)),
+                "dgsem_batch_set_launch_variant")
+
     def set_persistent(self, enable: bool = True) -> None:
         """One persistent launch per stage over all meshes (dgsem_batch_set_persistent)."""
         C.check(C.lib().dgsem_batch_set_persistent(self._h, int(enable)),

@@ -264,6 +264,10 @@ dgsem_status dgsem_batch_launch_count(const dgsem_batch* b, int64_t* count);
  * launches to rounding (the same body and tiles; bit for bit where the
  * compiler emits the same arithmetic).  DGSEM_ERR_UNSUPPORTED for other
  * batches.  Graphs record the mode they were captured in. */
+/* Selects one launch shape (dgsem_set_launch_variant's numbering) for every
+ * degree group of the batch, as dgsem_batch_autotune would after timing;
+ * DGSEM_ERR_INVALID_ARG if a group's scheme lacks it. */
+dgsem_status dgsem_batch_set_launch_variant(dgsem_batch* b, int variant);
 dgsem_status dgsem_batch_set_persistent(dgsem_batch* b, int enable);
 
 /* Hennemann-Gassner blending factor per element and troubled-cell flag

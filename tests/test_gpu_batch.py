@@ -139,3 +139,27 @@ def test_persistent_launch_equals_per_degree_launches(cuda):
     n0 = b.launch_count()
     b.step(0.0, dts)
     assert b.launch_count() - n0 == 3
+
+
+def test_batched_fixed_launch_variant(cuda):
+    """dgsem_batch_set_launch_variant: every launch shape of the batched
+    engines advances the batch like shape 0 (to rounding); a shape that a
+    degree group lacks is refused."""
+    import torch
+
+    from dgsem_b200 import _capi as C
+    dts = [1.4e-3] * len(SPECS)
+    ref = _batch(cuda)
+    ref.step(0.0, dts)
+    torch.cuda.synchronize()
+    ur = ref.u.cpu().numpy()
+    for v in (1, 2, 3, 4, 5):
+        b = _batch(cuda)
+        b.set_launch_variant(v)
+        b.step(0.0, dts)
+        torch.cuda.synchronize()
+        b.check_finite()
+        assert np.max(np.abs(b.u.cpu().numpy() - ur)) <= 1e-13 * np.max(np.abs(ur)), v
+    b = _batch(cuda)
+    with pytest.raises(C.DgsemError):
+        b.set_launch_variant(6)  # 2D engines have no shape 6
