@@ -100,11 +100,13 @@ def measured_peak():
 VARIANT_KERNELS = {
     0: "stage_kernel", 1: "stage_kernel", 2: "stage_kernel",
     3: "stage_node_kernel", 4: "stage_node_kernel", 5: "stage_pipe_kernel",
+    6: "stage_node2_kernel",
 }
 KERNEL_DESCRIPTIONS = {
     "stage_kernel": "stage_kernel (line-parallel fused RHS + SSPRK3 stage)",
     "stage_node_kernel": "stage_node_kernel (node-parallel fused RHS + SSPRK3 stage)",
     "stage_pipe_kernel": "stage_pipe_kernel (persistent node-parallel, TMA tile streaming)",
+    "stage_node2_kernel": "stage_node2_kernel (node-parallel, two nodes per thread)",
 }
 
 
@@ -856,7 +858,9 @@ def measure_batched(args):
         "ms_per_step_by_mode": mode_ms,
         "per_instance_ms_per_step_sum": plain_ms,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak,
+                     "traffic": profile_value("batched", "stage_node_kernel",
+                                              "traffic_bytes_per_stage"),
                      "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs"},
         "e2e": {"value": dofs * 3 / (statistics.mean(e2e) * 1e-3), "unit": "DOF-updates/s",
                 "h2d_bytes_per_step": dofs * 32, "d2h_bytes_per_step": dofs * 32},

@@ -123,7 +123,8 @@ struct StageArgs {
 // ---------------------------------------------------------------------------
 template <int DIM, int N>
 __device__ __forceinline__ void diag_add_node(const double* val, const BasisConst<N>& B, int node,
-                                              double inv_j, double gamma, double* acc) {
+                                              double inv_j, double gamma, double inv_gm1,
+                                              double* acc) {
   constexpr int NV = DIM + 2;
   const int in = node % N, jn = (node / N) % N, kn = node / (N * N);
   double wq = B.w[in] * B.w[jn];
@@ -134,7 +135,8 @@ __device__ __forceinline__ void diag_add_node(const double* val, const BasisCons
   for (int d = 0; d < DIM; ++d) m2 += val[1 + d] * val[1 + d];
   const double ke = 0.5 * m2 / val[0];
   const double p = (gamma - 1.0) * (val[NV - 1] - ke);
-  const double s = -val[0] * (log(p) - gamma * log(val[0])) / (gamma - 1.0);
+  // 1 / (gamma - 1) from the launch arguments: within an ulp of the division
+  const double s = -val[0] * (log(p) - gamma * log(val[0])) * inv_gm1;
   acc[0] += w;
   acc[1] += w * ke;
   acc[2] += w * s;
@@ -1096,7 +1098,7 @@ __device__ __forceinline__ void stage_body(const StageArgs<N>& p) {
       M.out[gi] = val;
       vals[q] = val;
     }
-    if (p.diag) diag_add_node<DIM, N>(vals, p.basis, node, -mij, gamma, dacc);
+    if (p.diag) diag_add_node<DIM, N>(vals, p.basis, node, -mij, gamma, p.inv_gm1, dacc);
   }
   if (bad) atomicOr(p.nonfinite, 1u);
   if constexpr (!BATCH) {

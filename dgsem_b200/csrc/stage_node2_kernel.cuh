@@ -249,7 +249,7 @@ __device__ __forceinline__ void stage_node2_body(const StageArgs<N>& p) {
         M.out[gi] = val;
         vals[q] = val;
       }
-      if (diag) diag_add_node<DIM, N>(vals, p.basis, node, -mij, gamma, dacc);
+      if (diag) diag_add_node<DIM, N>(vals, p.basis, node, -mij, gamma, p.inv_gm1, dacc);
     }
     if (bad) atomicOr(p.nonfinite, 1u);
   }

@@ -792,7 +792,7 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile 
     vals[q] = val;
   }
   if (bad) atomicOr(p.nonfinite, 1u);
-  if (diag) diag_add_node<DIM, N>(vals, p.basis, node, -mij, gamma, dacc);
+  if (diag) diag_add_node<DIM, N>(vals, p.basis, node, -mij, gamma, p.inv_gm1, dacc);
   }  // active
   // the state tile is free after the epilogue (it holds NV * NT >= 3 * NT doubles)
   if (diag) {

@@ -170,7 +170,7 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
         vals[q] = val;
       }
       if (bad) atomicOr(p.nonfinite, 1u);
-      if (p.diag) diag_add_node<DIM, N>(vals, p.basis, node, -mij, gamma, dacc);
+      if (p.diag) diag_add_node<DIM, N>(vals, p.basis, node, -mij, gamma, p.inv_gm1, dacc);
     }
     __syncthreads();
     // stage_n, shared tile, node data and face buffer are free again
