@@ -201,7 +201,12 @@ dgsem_status validate(const dgsem_mesh_desc* m, const dgsem_scheme_desc* s) {
     if (!(s->alpha_min >= 0.0 && s->alpha_max >= 0.0)) return DGSEM_ERR_INVALID_ARG;
   }
   if (ns) {
-    if (s->volume_integral != DGSEM_VI_SPLIT_FORM) return DGSEM_ERR_UNSUPPORTED;
+    // shock capturing with the viscous terms in 2D (the reference defines no
+    // 3D Navier-Stokes indicator)
+    if (s->volume_integral != DGSEM_VI_SPLIT_FORM &&
+        (m->ndims != 2 || s->volume_flux != DGSEM_VF_CHANDRASHEKAR ||
+         s->surface_flux != DGSEM_SF_LAX_FRIEDRICHS))
+      return DGSEM_ERR_UNSUPPORTED;
     // periodic directions or (2D) the Navier-Stokes adiabatic walls; 3D
     // meshes are periodic (checked above)
     for (int f = 0; f < 2 * m->ndims; ++f)
@@ -583,7 +588,7 @@ dgsem_status dgsem_graph_destroy(dgsem_graph* g) {
 dgsem_status dgsem_indicator(dgsem_ctx* ctx, const double* u, double* alpha,
                              uint8_t* flags) {
   if (!ctx || !u) return DGSEM_ERR_INVALID_ARG;
-  if (is_navier_stokes(ctx->scheme.equation)) return DGSEM_ERR_UNSUPPORTED;
+  if (ctx->scheme.equation == DGSEM_NAVIER_STOKES_3D) return DGSEM_ERR_UNSUPPORTED;
   const EngineConfig& c = ctx->cfg;
   const int threads = 128;
   const unsigned blocks = (unsigned)((c.nelem + threads - 1) / threads);

@@ -183,10 +183,10 @@ class Engine final : public EngineBase {
  public:
   static constexpr int GRAD_EPB = (128 / ipow(N, DIM)) > 0 ? (128 / ipow(N, DIM)) : 1;
   static constexpr bool kBatch = !NS && !HG;
-  // the line-parallel shapes 0-2 carry shock capturing and the viscous terms
-  // in 2D only; in 3D these run on the node-parallel shapes (0-2 then run
-  // shape 3)
-  static constexpr bool kLine = !(DIM == 3 && (HG || NS));
+  // the line-parallel shapes 0-2 carry shock capturing or the viscous terms
+  // in 2D only (not both); otherwise the node-parallel shapes run (0-2 then
+  // run shape 3)
+  static constexpr bool kLine = !(DIM == 3 && (HG || NS)) && !(HG && NS);
 
   template <int V>
   using Sh = StageShape<DIM, N, VF, SF, HG, LaunchShape<DIM, N, V>::EPB, NS>;

@@ -496,7 +496,8 @@ __device__ __forceinline__ void node_face_tasks(const StageArgs<N>& p, const Mes
 template <int DIM, int N, int VF, int SF, int EPB, bool BATCH, bool HG, bool NS = false,
           int NTB = 0, bool PERSIST = false>
 __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile = 0) {
-  static_assert(!NS || (!HG && !BATCH), "Navier-Stokes: split form, single mesh");
+  static_assert(!NS || (!BATCH && (!HG || DIM == 2)),
+                "Navier-Stokes: single mesh; with shock capturing in 2D");
   using S = NodeShape<DIM, N, VF, EPB, HG, NS>;
   using K = NodeKernelSlots<DIM, VF>;
   constexpr int NV = S::NV, ND = S::ND, NDP = S::NDP, NF = S::NF, NFACE = S::NFACE,
@@ -699,49 +700,6 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile 
       node_volume_direction<2, DIM, N, VF, NDP, WARP_ALL, S::XCHG>(p, M, U, P, I, node, pn, own,
                                                                   hgm1, acc, xbuf, tid, NT,
                                                                   worker);
-    if constexpr (NS && DIM == 3) {
-      // viscous weak-form volume term sum_k Dhat(m, k) Ja^dir(k) . (-F_v)(k)
-      // along each line through the node (parabolic_viscous.hpp:398-469)
-      const double* W = wv + ev * 3 * NV * ND;
-#pragma unroll
-      for (int dir = 0; dir < 3; ++dir) {
-        const int m = dir == 0 ? node % N : dir == 1 ? (node / N) % N : node / (N * N);
-        const int stride = dir == 0 ? 1 : dir == 1 ? N : N * N;
-        const double* j0 = M.tab.ja[dir][0] + (int64_t)I[3] * ND;
-        const double* j1 = M.tab.ja[dir][1] + (int64_t)I[4] * ND;
-        const double* j2 = M.tab.ja[dir][2] + (int64_t)I[5] * ND;
-#pragma unroll
-        for (int k = 0; k < N; ++k) {
-          const int nk = node + (k - m) * stride;
-          const double a0 = __ldg(j0 + nk), a1 = __ldg(j1 + nk), a2 = __ldg(j2 + nk);
-          const double dmk = p.basis.Dhat[m][k];
-#pragma unroll
-          for (int q = 0; q < NV; ++q)
-            acc[q] += dmk * (a0 * W[(0 * NV + q) * ND + nk] + a1 * W[(1 * NV + q) * ND + nk] +
-                             a2 * W[(2 * NV + q) * ND + nk]);
-        }
-      }
-    } else if constexpr (NS) {
-      // viscous weak-form volume term sum_k Dhat(m, k) Ja^dir(k) . (-F_v)(k)
-      // along each line through the node (parabolic_viscous.hpp:418-466)
-      const double* W = wv + ev * 2 * NV * ND;
-#pragma unroll
-      for (int dir = 0; dir < 2; ++dir) {
-        const int m = dir == 0 ? node % N : node / N;
-        const int stride = dir == 0 ? 1 : N;
-        const double* j0 = M.tab.ja[dir][0] + (int64_t)I[3] * ND;
-        const double* j1 = M.tab.ja[dir][1] + (int64_t)I[4] * ND;
-#pragma unroll
-        for (int k = 0; k < N; ++k) {
-          const int nk = node + (k - m) * stride;
-          const double a0 = __ldg(j0 + nk), a1 = __ldg(j1 + nk);
-          const double dmk = p.basis.Dhat[m][k];
-#pragma unroll
-          for (int q = 0; q < NV; ++q)
-            acc[q] += dmk * (a0 * W[(0 * NV + q) * ND + nk] + a1 * W[(1 * NV + q) * ND + nk]);
-        }
-      }
-    }
   }
   if constexpr (HG) {
     if (active) {
@@ -758,6 +716,58 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile 
         node_fv_direction<1, DIM, N, VF, NDP>(p, M, U, P, I, node, alpha, acc);
         if constexpr (DIM == 3)
           node_fv_direction<2, DIM, N, VF, NDP>(p, M, U, P, I, node, alpha, acc);
+      }
+    }
+  }
+  // viscous terms after the shock-capturing blend: the blend covers the
+  // inviscid volume integral only (the reference adds the parabolic terms
+  // separately, structured_solver.hpp:437-480)
+  if constexpr (NS) {
+    if (active) {
+      const int ev = el;
+      const int* I = info + el * NI;
+      if constexpr (NS && DIM == 3) {
+        // viscous weak-form volume term sum_k Dhat(m, k) Ja^dir(k) . (-F_v)(k)
+        // along each line through the node (parabolic_viscous.hpp:398-469)
+        const double* W = wv + ev * 3 * NV * ND;
+#pragma unroll
+        for (int dir = 0; dir < 3; ++dir) {
+          const int m = dir == 0 ? node % N : dir == 1 ? (node / N) % N : node / (N * N);
+          const int stride = dir == 0 ? 1 : dir == 1 ? N : N * N;
+          const double* j0 = M.tab.ja[dir][0] + (int64_t)I[3] * ND;
+          const double* j1 = M.tab.ja[dir][1] + (int64_t)I[4] * ND;
+          const double* j2 = M.tab.ja[dir][2] + (int64_t)I[5] * ND;
+#pragma unroll
+          for (int k = 0; k < N; ++k) {
+            const int nk = node + (k - m) * stride;
+            const double a0 = __ldg(j0 + nk), a1 = __ldg(j1 + nk), a2 = __ldg(j2 + nk);
+            const double dmk = p.basis.Dhat[m][k];
+#pragma unroll
+            for (int q = 0; q < NV; ++q)
+              acc[q] += dmk * (a0 * W[(0 * NV + q) * ND + nk] + a1 * W[(1 * NV + q) * ND + nk] +
+                               a2 * W[(2 * NV + q) * ND + nk]);
+          }
+        }
+      } else if constexpr (NS) {
+        // viscous weak-form volume term sum_k Dhat(m, k) Ja^dir(k) . (-F_v)(k)
+        // along each line through the node (parabolic_viscous.hpp:418-466)
+        const double* W = wv + ev * 2 * NV * ND;
+#pragma unroll
+        for (int dir = 0; dir < 2; ++dir) {
+          const int m = dir == 0 ? node % N : node / N;
+          const int stride = dir == 0 ? 1 : N;
+          const double* j0 = M.tab.ja[dir][0] + (int64_t)I[3] * ND;
+          const double* j1 = M.tab.ja[dir][1] + (int64_t)I[4] * ND;
+#pragma unroll
+          for (int k = 0; k < N; ++k) {
+            const int nk = node + (k - m) * stride;
+            const double a0 = __ldg(j0 + nk), a1 = __ldg(j1 + nk);
+            const double dmk = p.basis.Dhat[m][k];
+#pragma unroll
+            for (int q = 0; q < NV; ++q)
+              acc[q] += dmk * (a0 * W[(0 * NV + q) * ND + nk] + a1 * W[(1 * NV + q) * ND + nk]);
+          }
+        }
       }
     }
   }

@@ -43,7 +43,10 @@ def ns_combos():
     # 2D Navier-Stokes (BR1, periodic or walls): n in 2..8, the three volume
     # fluxes, LLF; 3D Navier-Stokes (periodic): n in 2..5, the three volume
     # fluxes, LLF (node-parallel shapes).
+    # 2D Navier-Stokes with Hennemann-Gassner shock capturing (the
+    # reference's viscous KHI setup): Chandrashekar / LLF, n in 2..8.
     return (sorted((2, n, vf, 0, 0, 1) for n in range(2, 9) for vf in range(3)) +
+            sorted((2, n, 0, 0, 1, 1) for n in range(2, 9)) +
             sorted((3, n, vf, 0, 0, 1) for n in range(2, 6) for vf in range(3)))
 
 

@@ -35,8 +35,9 @@ EULER2D_CURVED_CENTRAL = 7     # curvilinear periodic mesh, CentralFlux + LLF (p
 EULER3D_CURVED = 8             # curvilinear periodic mesh, Chandrashekar + LLF (polydeg <= 4)
 NS2D_CHANNEL_WALLS = 9         # Navier-Stokes, x periodic, no-slip bottom / slip top wall
 NS3D_PERIODIC_SPLIT = 10       # 3D Navier-Stokes BR1 + Chandrashekar/LLF, periodic (polydeg <= 4)
+NS2D_PERIODIC_HG = 11          # 2D Navier-Stokes + HG shock capturing, periodic (viscous KHI)
 
-_DIMS = {0: 2, 1: 2, 2: 2, 3: 3, 4: 3, 5: 2, 6: 2, 7: 2, 8: 3, 9: 2, 10: 3}
+_DIMS = {0: 2, 1: 2, 2: 2, 3: 3, 4: 3, 5: 2, 6: 2, 7: 2, 8: 3, 9: 2, 10: 3, 11: 2}
 
 
 class _Case(ctypes.Structure):

@@ -49,6 +49,7 @@ enum {
   REF_EULER3D_CURVED = 8,             // curvilinear periodic mesh, Chandrashekar + LLF
   REF_NS2D_CHANNEL_WALLS = 9,         // NS, x periodic, no-slip bottom / slip top walls
   REF_NS3D_PERIODIC_SPLIT = 10,       // 3D Navier-Stokes BR1 + split form, periodic box
+  REF_NS2D_PERIODIC_HG = 11,          // 2D Navier-Stokes + HG shock capturing (viscous KHI)
 };
 
 typedef struct {
@@ -616,6 +617,13 @@ RefCaseBase* make_case_n(const dgsem_ref_case& c) {
       auto b = DGSEM::BoundarySet(P{}, P{}, P{}, P{});
       return new RefCase<NS2, N, VF, decltype(b), 2>(
           c, NS2{c.gamma, c.mu, c.prandtl}, b, true);
+    }
+    case REF_NS2D_PERIODIC_HG: {
+      using VF = DGSEM::VolumeIntegralShockCapturingHG<Basis, NS2, DGSEM::ChandrashekarFlux,
+                                                       DGSEM::LaxFriedrichsFlux,
+                                                       DGSEM::HGIndicator<Basis, NS2>>;
+      auto b = DGSEM::BoundarySet(P{}, P{}, P{}, P{});
+      return new RefCase<NS2, N, VF, decltype(b), 2>(c, NS2{c.gamma, c.mu, c.prandtl}, b, true);
     }
     case REF_NS3D_PERIODIC_SPLIT: {
       if constexpr (N <= 4) {
