@@ -12,7 +12,7 @@
 //   DGSEM::Solution<Mesh, Basis, Eq>                  solution_container.hpp:157-234
 //   DGSEM::SSPRK3<T, Solver, Mesh, Solution>          SSPRK3.hpp:145-187
 //     ::step / ::solve / ::add_observer / ::get_time  integrator_base.hpp:15-47
-//   plugins: equations::CompressibleEuler2D/3D, CompressibleNavierStokes2D;
+//   plugins: equations::CompressibleEuler2D/3D, CompressibleNavierStokes2D/3D;
 //     ChandrashekarFlux (+ RanochaFlux, KennedyGruberFlux), LaxFriedrichsFlux,
 //     HLLCFlux (2D); VolumeIntegralSplitForm, VolumeIntegralShockCapturingHG
 //     with HGIndicator; PeriodicBC, OutflowBC, SlipWallBC, DirichletBC,
@@ -132,6 +132,18 @@ struct CompressibleNavierStokes2D {
   static constexpr int dgsem_code = DGSEM_NAVIER_STOKES_2D;
   T gamma = T(1.4);
   T mu = T(0);
+  T prandtl = T(0.72);
+  T get_gamma() const { return gamma; }
+  T viscosity() const { return mu; }
+  T prandtl_number() const { return prandtl; }
+};
+// equations/compressible_navier_stokes3D.hpp (periodic boxes)
+template <class T>
+struct CompressibleNavierStokes3D {
+  static constexpr std::size_t NDIMS = 3, NVARS = 5;
+  static constexpr int dgsem_code = DGSEM_NAVIER_STOKES_3D;
+  T gamma = T(1.4);
+  T mu = T(6.25e-4);
   T prandtl = T(0.72);
   T get_gamma() const { return gamma; }
   T viscosity() const { return mu; }
