@@ -746,12 +746,28 @@ def batched_config() -> dict:
 
 
 def run_batched(args):
-    """Batched multi-mesh throughput and speedup over the per-instance path."""
-    print(json.dumps(measure_batched(args)))
+    """Batched multi-mesh throughput and speedup over the per-instance path.
+    With N ranks (one per GPU, no data-path collective: meshes never
+    exchange data): by default every rank advances its own 256-mesh batch
+    (seed + rank; weak scaling); with --shard-meshes the one 256-mesh batch
+    is split over the ranks by cost (dgsem_b200.sharding; strong scaling)."""
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    line = measure_batched(args, rank, world)
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
     return 0
 
 
-def measure_batched(args):
+def measure_batched(args, rank: int = 0, world: int = 1):
     """The batched line (see run_batched)."""
     import ctypes
 
@@ -759,9 +775,17 @@ def measure_batched(args):
 
     import dgsem_b200 as D
     from dgsem_b200 import _capi as C
+    from dgsem_b200 import sharding
 
     dev = torch.device("cuda", torch.cuda.current_device())
-    specs = batched_meshes()
+    shard = world > 1 and getattr(args, "shard_meshes", False)
+    if shard:
+        job = batched_meshes()
+        specs = [s for _, s in sharding.local_meshes(job, rank, world)]
+        job_dofs = sum(cells[0] * cells[1] * (N + 1) ** 2 for cells, N, _, _ in job)
+    else:
+        specs = batched_meshes(seed=20260512 + rank)
+        job_dofs = None
     eq = D.CompressibleEuler2D(1.4)
     meshes = [(D.StructuredMesh((-5.0, -5.0), (5.0, 5.0), cells), N) for cells, N, _, _ in specs]
     # dt = CFL 0.5 * dx / ((2n - 1) * lambda_max), lambda_max <= 4 for these vortices
@@ -806,8 +830,12 @@ def measure_batched(args):
     mode = min(mode_ms, key=mode_ms.get)
     step_ms, launches, clocks, g = modes[mode]
     batch.set_persistent(mode == "persistent")
-    total_ms = sum(step_ms)
-    value = dofs * 3 * args.steps / (total_ms * 1e-3)
+    # the job's time is the slowest rank's (max over ranks)
+    total_ms = max_over_ranks(sum(step_ms), world, dev)
+    if shard:
+        value = job_dofs * 3 * args.steps / (total_ms * 1e-3)
+    else:
+        value = aggregate_rate(world, dofs, args.steps, total_ms)
     # per-instance plain path: one solver per mesh, 3 stage launches per step
     per_ms = []
     for k, (cells, N, beta, c) in enumerate(specs):
@@ -831,7 +859,7 @@ def measure_batched(args):
             torch.cuda.synchronize()
         per_ms.append(a.elapsed_time(b) / 3.0)
         del solver, sol, integ
-    plain_ms = sum(per_ms)
+    plain_ms = max_over_ranks(sum(per_ms), world, dev)
     batched_ms = total_ms / args.steps
     # e2e: pinned host state in, one batched step, state out
     host = batch.u.detach().to("cpu").pin_memory()
@@ -843,13 +871,20 @@ def measure_batched(args):
         host.copy_(batch.u, non_blocking=True)
         torch.cuda.synchronize()
         e2e.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = max_over_ranks(statistics.mean(e2e), world, dev)
+    e2e_dofs = job_dofs if shard else world * dofs
+    # per GPU: this rank's bytes in the job's (slowest rank's) stage time
     bytes_stage = dofs * bytes_per_dof_stage(4)
     achieved = bytes_stage / (batched_ms / 3.0 * 1e-3) / 1e9
     peak, peak_kind = measured_peak()
     line = {
         "metric": "FP64 DOF-updates/s per RHS (batched)", "value": value,
-        "unit": "DOF-updates/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": batched_ms, "higher_is_better": True, "scaling": "weak",
+        "unit": "DOF-updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": batched_ms, "higher_is_better": True,
+        "scaling": "strong" if shard else "weak",
+        "parallelism": (f"the 256 meshes split over {world} ranks by cost (no collective)"
+                        if shard else f"{world} ranks, each its own 256-mesh batch"
+                        if world > 1 else "single"),
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded isentropic vortices)",
         "config": batched_config(),
         "launch_variants": variants,
@@ -862,7 +897,7 @@ def measure_batched(args):
                      "traffic": profile_value("batched", "stage_node_kernel",
                                               "traffic_bytes_per_stage"),
                      "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs"},
-        "e2e": {"value": dofs * 3 / (statistics.mean(e2e) * 1e-3), "unit": "DOF-updates/s",
+        "e2e": {"value": e2e_dofs * 3 / (e2e_ms * 1e-3), "unit": "DOF-updates/s",
                 "h2d_bytes_per_step": dofs * 32, "d2h_bytes_per_step": dofs * 32},
         "gpu_launches": launches, "clocks": clocks,
     }
@@ -1023,6 +1058,9 @@ def main():
     ap.add_argument("--workload", default="tgv16",
                     choices=list(WORKLOADS) + ["batched", "adjoint"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shard-meshes", action="store_true",
+                    help="batched workload on N GPUs: split the one 256-mesh batch over the "
+                         "ranks by cost (strong scaling) instead of a batch per rank")
     ap.add_argument("--no-side-workloads", action="store_true",
                     help="skip the short batched / adjoint runs recorded in details")
     ap.add_argument("--variant", default="auto", choices=["auto", "0", "1", "2", "3", "4", "5", "6"],
