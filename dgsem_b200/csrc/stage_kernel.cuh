@@ -487,29 +487,44 @@ __device__ __forceinline__ void stage_dependency_sync() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
-// Copies the u tile [el][var][node] of `ne` elements from `src` (global) to
-// the padded shared layout `us`.  For a full tile (ne == EPB) each thread
-// issues all of its loads before its first store, so the block waits for one
-// global round trip instead of one per loop iteration.
+// The u tile [el][var][node] of a block in two steps: issue() starts every
+// global load of this thread for a full tile (ne == EPB) into registers,
+// store() writes them to the padded shared layout `us` (a partial tile is
+// loaded and stored in store()).  Work placed between the two overlaps the
+// loads' latency, and the block waits for one global round trip instead of
+// one per loop iteration.
 template <int N, int NV, int ND, int NDP, int EPB, int NT>
-__device__ __forceinline__ void load_element_tile(const double* src, double* us, int ne,
-                                                  int tid) {
-  constexpr int TILE = EPB * NV * ND, PER = (TILE + NT - 1) / NT;
-  constexpr bool PAD = NDP != ND;
-  if (ne == EPB) {
-    double v[PER];
+struct ElementTileLoad {
+  static constexpr int TILE = EPB * NV * ND, PER = (TILE + NT - 1) / NT;
+  static constexpr bool PAD = NDP != ND;
+  double v[PER];
+  __device__ __forceinline__ void issue(const double* src, int ne, int tid) {
+    if (ne != EPB) return;
 #pragma unroll
     for (int r = 0; r < PER; ++r)
       if (TILE % NT == 0 || tid + r * NT < TILE) v[r] = __ldg(src + tid + r * NT);
-#pragma unroll
-    for (int r = 0; r < PER; ++r) {
-      const int idx = tid + r * NT;
-      if (TILE % NT == 0 || idx < TILE) us[(idx / ND) * NDP + padn<N, PAD>(idx % ND)] = v[r];
-    }
-  } else {
-    for (int idx = tid; idx < ne * NV * ND; idx += NT)
-      us[(idx / ND) * NDP + padn<N, PAD>(idx % ND)] = __ldg(src + idx);
   }
+  __device__ __forceinline__ void store(const double* src, double* us, int ne, int tid) const {
+    if (ne == EPB) {
+#pragma unroll
+      for (int r = 0; r < PER; ++r) {
+        const int idx = tid + r * NT;
+        if (TILE % NT == 0 || idx < TILE) us[(idx / ND) * NDP + padn<N, PAD>(idx % ND)] = v[r];
+      }
+    } else {
+      for (int idx = tid; idx < ne * NV * ND; idx += NT)
+        us[(idx / ND) * NDP + padn<N, PAD>(idx % ND)] = __ldg(src + idx);
+    }
+  }
+};
+
+// issue() and store() back to back.
+template <int N, int NV, int ND, int NDP, int EPB, int NT>
+__device__ __forceinline__ void load_element_tile(const double* src, double* us, int ne,
+                                                  int tid) {
+  ElementTileLoad<N, NV, ND, NDP, EPB, NT> t;
+  t.issue(src, ne, tid);
+  t.store(src, us, ne, tid);
 }
 
 // Per-node shared-memory slots: the velocity, the flux-specific scalars and

@@ -154,7 +154,12 @@ __device__ __forceinline__ void stage_node2_body(const StageArgs<N>& p) {
   const double t_stage = p.t_dev ? (*p.t_dev + p.t) : p.t;
   const int c0 = M.cells[0], c1 = M.cells[1], c2 = M.cells[2];
 
-  // the epilogue's u_n tile: one bulk copy requested now (block-uniform)
+  // ---- phase 0: the u_in tile, the epilogue's u_n tile, element info ----
+  // (issue order as in stage_node_body: u_in loads, the u_n bulk copy, the
+  // element info while the loads are in flight, then the tile store)
+  const double* tile_src = M.u_in + (int64_t)e0 * NV * ND;
+  ElementTileLoad<N, NV, ND, NDP, EPB, NT> tload;
+  tload.issue(tile_src, ne, tid);
   __shared__ uint64_t bar_n;
   bool bulk_n = false;
   if constexpr (S::SM_N > 0)
@@ -166,10 +171,8 @@ __device__ __forceinline__ void stage_node2_body(const StageArgs<N>& p) {
     mbar_arrive_expect_tx(&bar_n, bytes);
     if (!p.skip_tile_copy) bulk_copy_g2s(stage_n, M.u_n + (int64_t)e0 * NV * ND, bytes, &bar_n);
   }
-
-  // ---- phase 0: element info and the u_in tile --------------------------
   node_element_info<DIM, NI>(M, info, e0, ne, tid, NT);
-  load_element_tile<N, NV, ND, NDP, EPB, NT>(M.u_in + (int64_t)e0 * NV * ND, us, ne, tid);
+  tload.store(tile_src, us, ne, tid);
   __syncthreads();
 
   // ---- phase 1: node data of both nodes ----------------------------------

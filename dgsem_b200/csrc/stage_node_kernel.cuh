@@ -536,8 +536,14 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile 
   const double t_stage = p.t_dev ? (*p.t_dev + p.t) : p.t;
   const int c0 = M.cells[0], c1 = M.cells[1], c2 = M.cells[2];
 
-  // The epilogue's u_n tile is requested now as one bulk copy so that it
-  // arrives while the block computes (block-uniform decision).
+  // ---- phase 0: the u_in tile, the epilogue's u_n tile, element info ----
+  // The u_in loads are issued first; the u_n tile is requested as one bulk
+  // copy that arrives while the block computes (block-uniform decision); the
+  // element info is computed while the u_in loads are in flight, then the
+  // tile is stored to shared memory.
+  const double* tile_src = M.u_in + (int64_t)e0 * NV * ND;
+  ElementTileLoad<N, NV, ND, NDP, EPB, NT> tload;
+  if (worker) tload.issue(tile_src, ne, tid);
   __shared__ uint64_t bar_n;
   bool bulk_n = false;
   if constexpr (S::SM_N > 0 && !PERSIST)
@@ -549,14 +555,11 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile 
     mbar_arrive_expect_tx(&bar_n, bytes);
     if (!p.skip_tile_copy) bulk_copy_g2s(stage_n, M.u_n + (int64_t)e0 * NV * ND, bytes, &bar_n);
   }
-
-  // ---- phase 0: element info and the u_in tile --------------------------
   node_element_info<DIM, NI>(M, info, e0, ne, tid, NT);
   if constexpr (HG) {
     for (int k = tid; k < N * N; k += NT) vinv_s[k] = p.basis.Vinv[k / N][k % N];
   }
-  if (worker)
-    load_element_tile<N, NV, ND, NDP, EPB, NT>(M.u_in + (int64_t)e0 * NV * ND, us, ne, tid);
+  if (worker) tload.store(tile_src, us, ne, tid);
   __syncthreads();
 
   // ---- phase 1: node data, squared sound speed and -1/J ------------------
