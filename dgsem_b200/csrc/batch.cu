@@ -423,6 +423,8 @@ dgsem_status dgsem_batch_create(const dgsem_mesh_desc* meshes, int n_meshes,
     c.basis = bases[g.n];
     c.nonfinite = b->flag;
     c.grad = nullptr;
+    c.elem_info = nullptr;  // batched launches compute the element info in the kernel
+    c.mij = nullptr;
     for (int f = 0; f < 6; ++f) c.bc.kind[f] = 0;
     g.members = kv.second;
     // tile arrays sized for one element per tile (any launch shape fits)

@@ -386,6 +386,17 @@ dgsem_status dgsem_ctx_create(const dgsem_mesh_desc* mesh,
     c.grad = device_alloc<double>(ctx, (size_t)c.nelem * 4 * nd * ctx->nodes, &err);
     if (!c.grad) ctx->flag = nullptr;
   }
+  // per-element info and -1/J per node, computed once here instead of in
+  // every stage launch
+  c.elem_info = nullptr;
+  c.mij = nullptr;
+  int* info_tab = nullptr;
+  double* mij_tab = nullptr;
+  if (ctx->flag) {
+    info_tab = device_alloc<int>(ctx, (size_t)c.nelem * 12, &err);
+    mij_tab = info_tab ? device_alloc<double>(ctx, (size_t)c.nelem * ctx->nodes, &err) : nullptr;
+    if (!mij_tab) ctx->flag = nullptr;
+  }
   if (!ctx->flag) {
     free_all(ctx);
     delete ctx;
@@ -393,7 +404,12 @@ dgsem_status dgsem_ctx_create(const dgsem_mesh_desc* mesh,
   }
   cudaMemset(ctx->flag, 0, sizeof(unsigned int));
   c.nonfinite = ctx->flag;
-  err = cudaDeviceSynchronize();
+  err = ctx->engine->build_mesh_tables(c, info_tab, mij_tab, nullptr);
+  if (err == cudaSuccess) {
+    c.elem_info = info_tab;
+    c.mij = mij_tab;
+  }
+  if (err == cudaSuccess) err = cudaDeviceSynchronize();
   if (err != cudaSuccess) {
     free_all(ctx);
     delete ctx;

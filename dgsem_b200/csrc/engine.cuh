@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <memory>
 #include <utility>
 
@@ -37,6 +38,10 @@ struct EngineConfig {
   BasisTables basis;
   unsigned int* nonfinite;  // device flag
   double* grad;             // Navier-Stokes lifted gradient [E][4][2][n^2]
+  // per-element info (node_element_info layout, 12 ints per element) and
+  // -1/J per node [E][n^d], computed once per context (may be null)
+  const int* elem_info;
+  const double* mij;
   // failure-path testing (StageArgs::wait_limit_ns / skip_tile_copy)
   unsigned long long wait_limit_ns;
   int skip_tile_copy;
@@ -44,9 +49,10 @@ struct EngineConfig {
 
 // Launch-shape variants: 0-2 line-parallel (stage_kernel.cuh), 3-4
 // node-parallel (stage_node_kernel.cuh), 5 persistent node-parallel with TMA
-// tile streaming (stage_pipe_kernel.cuh; single-mesh launches).  3-5 cover
-// the split form without shock capturing or viscous terms; 5 needs an even
-// number of doubles per element (2D, or 3D with even n).
+// tile streaming (stage_pipe_kernel.cuh; single-mesh launches; split form
+// without shock capturing or viscous terms, an even number of doubles per
+// element), 6 two nodes per thread (stage_node2_kernel.cuh; 3D, n = 2 or 4,
+// split form without shock capturing or viscous terms).
 constexpr int kNumVariants = 7;
 
 class EngineBase {
@@ -61,6 +67,10 @@ class EngineBase {
                             double* alpha_out, cudaStream_t s, double* diag = nullptr) = 0;
   // number of diag slots (blocks) the last stage launch with diag wrote
   virtual int64_t last_diag_slots() const = 0;
+  // Fills the per-mesh tables of the node-parallel kernels (EngineConfig::
+  // elem_info, 12 ints per element; ::mij, -1/J per node) on stream s.
+  virtual cudaError_t build_mesh_tables(const EngineConfig& cfg, int* info, double* mij,
+                                        cudaStream_t s) const = 0;
   // Batched launch over a tile list (mesh index and first element per block)
   // of meshes sharing this engine's scheme and degree; per-mesh data in
   // `meshes` (device array).  Tiles are built with elements_per_block().
@@ -357,6 +367,8 @@ class Engine final : public EngineBase {
     }
     args.mesh.nelem = (int)cfg.nelem;
     args.mesh.tab = cfg.tab;
+    args.mesh.info = cfg.elem_info;
+    args.mesh.mij = cfg.mij;
     if constexpr (NS) {
       GradArgs<N> ga{};
       ga.u = u_in;
@@ -419,6 +431,21 @@ class Engine final : public EngineBase {
       }
       return cudaGetLastError();
     }
+  }
+
+  cudaError_t build_mesh_tables(const EngineConfig& cfg, int* info, double* mij,
+                                cudaStream_t s) const override {
+    MeshView m{};
+    for (int i = 0; i < 3; ++i) {
+      m.cells[i] = (int)cfg.cells[i];
+      m.periodic[i] = cfg.periodic[i];
+    }
+    m.nelem = (int)cfg.nelem;
+    m.tab = cfg.tab;
+    const int64_t nodes = cfg.nelem * ipow(N, DIM);
+    const unsigned blocks = (unsigned)std::min<int64_t>((nodes + 255) / 256, 4096);
+    element_tables_kernel<DIM, N, 12><<<blocks, 256, 0, s>>>(m, info, mij);
+    return cudaGetLastError();
   }
 
   int kernels_per_stage() const override { return NS ? 2 : 1; }

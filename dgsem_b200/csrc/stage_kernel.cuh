@@ -83,6 +83,10 @@ struct MeshView {
   int nelem;
   int periodic[3];
   DeviceTables tab;
+  // optional per-mesh tables of the node-parallel kernels (null: computed in
+  // the kernel): element info, 12 ints per element, and -1/J per node
+  const int* info;
+  const double* mij;
 };
 
 template <int N>

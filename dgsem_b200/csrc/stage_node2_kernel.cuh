@@ -160,6 +160,15 @@ __device__ __forceinline__ void stage_node2_body(const StageArgs<N>& p) {
   const double* tile_src = M.u_in + (int64_t)e0 * NV * ND;
   ElementTileLoad<N, NV, ND, NDP, EPB, NT> tload;
   tload.issue(tile_src, ne, tid);
+  const int el = tid / NH, h = tid % NH;
+  const int nA = h, nB = h + NH;
+  const bool active = el < ne;
+  // -1/J of the two nodes from the mesh's table, requested with the tile
+  double mij_ab[2] = {0.0, 0.0};
+  if (M.mij && active) {
+    mij_ab[0] = __ldg(M.mij + (int64_t)(e0 + el) * ND + nA);
+    mij_ab[1] = __ldg(M.mij + (int64_t)(e0 + el) * ND + nB);
+  }
   __shared__ uint64_t bar_n;
   bool bulk_n = false;
   if constexpr (S::SM_N > 0)
@@ -171,14 +180,15 @@ __device__ __forceinline__ void stage_node2_body(const StageArgs<N>& p) {
     mbar_arrive_expect_tx(&bar_n, bytes);
     if (!p.skip_tile_copy) bulk_copy_g2s(stage_n, M.u_n + (int64_t)e0 * NV * ND, bytes, &bar_n);
   }
-  node_element_info<DIM, NI>(M, info, e0, ne, tid, NT);
+  if (M.info) {
+    for (int k = tid; k < ne * NI; k += NT) info[k] = __ldg(M.info + (int64_t)e0 * NI + k);
+  } else {
+    node_element_info<DIM, NI>(M, info, e0, ne, tid, NT);
+  }
   tload.store(tile_src, us, ne, tid);
   __syncthreads();
 
   // ---- phase 1: node data of both nodes ----------------------------------
-  const int el = tid / NH, h = tid % NH;
-  const int nA = h, nB = h + NH;
-  const bool active = el < ne;
   if (active) {
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
@@ -186,7 +196,8 @@ __device__ __forceinline__ void stage_node2_body(const StageArgs<N>& p) {
       double u[NV];
 #pragma unroll
       for (int q = 0; q < NV; ++q) u[q] = us[(el * NV + q) * NDP + node];
-      node_prepare<DIM, N, VF, NDP>(M, u, gamma, info + el * NI, node, pr + el * NQ * NDP + node);
+      node_prepare<DIM, N, VF, NDP>(M, u, gamma, info + el * NI, node, pr + el * NQ * NDP + node,
+                                    M.mij ? &mij_ab[s] : nullptr);
     }
   }
   __syncthreads();

@@ -377,12 +377,49 @@ __device__ __forceinline__ void node_element_info(const MeshView& M, int* info, 
   }
 }
 
+// -1/J of a node from the separable tables: 1/J = 1/(J00 J11 [J22]) (the
+// off-diagonal products do not change the rounded determinant).
+template <int DIM, int N>
+__device__ __forceinline__ double node_minus_inv_j(const DeviceTables& tab, int i0, int i1,
+                                                   int i2, int in, int jn, int kn) {
+  double jdet = __ldg(tab.jdiag[0] + i0 * N + in);
+  if (DIM == 2) {
+    jdet = jdet * __ldg(tab.jdiag[1] + i1 * N + jn);
+  } else {
+    jdet = jdet * (__ldg(tab.jdiag[1] + i1 * N + jn) * __ldg(tab.jdiag[2] + i2 * N + kn));
+  }
+  return -(1.0 / jdet);
+}
+
+// The per-mesh tables of the node-parallel kernels (MeshView::info, ::mij),
+// once per context: every element's info entries (node_element_info) and
+// -1/J of every node.  One thread per (element, node).
+template <int DIM, int N, int NI>
+__global__ void element_tables_kernel(const MeshView M, int* info, double* mij) {
+  constexpr int ND = ipow(N, DIM);
+  const int64_t total = (int64_t)M.nelem * ND;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += stride) {
+    const int e = (int)(g / ND), node = (int)(g % ND);
+    const int c0 = M.cells[0], c1 = M.cells[1];
+    const int i0 = e % c0;
+    const int i1 = DIM == 2 ? e / c0 : (e / c0) % c1;
+    const int i2 = DIM == 2 ? 0 : e / (c0 * c1);
+    const int in = node % N, jn = (node / N) % N, kn = DIM == 3 ? node / (N * N) : 0;
+    mij[g] = node_minus_inv_j<DIM, N>(M.tab, i0, i1, i2, in, jn, kn);
+  }
+  // element info: the tile function over all elements as one tile
+  node_element_info<DIM, NI>(M, info, 0, M.nelem, (int)(blockIdx.x * blockDim.x + threadIdx.x),
+                             (int)(gridDim.x * blockDim.x));
+}
+
 // Per-node data of phase 1 (NodeKernelSlots) from the conserved state u:
 // the (halved) primitive variables, the squared sound speed gamma p / rho and
 // -1/J from the separable metric tables.
 template <int DIM, int N, int VF, int NDP>
 __device__ __forceinline__ void node_prepare(const MeshView& M, const double* u, double gamma,
-                                             const int* I, int node, double* P) {
+                                             const int* I, int node, double* P,
+                                             const double* mij_pre = nullptr) {
   using K = NodeKernelSlots<DIM, VF>;
   const NodeState<DIM> s = prepare_node<DIM, VF>(u, gamma);
   const double h = K::HALF ? 0.5 : 1.0;
@@ -397,14 +434,12 @@ __device__ __forceinline__ void node_prepare(const MeshView& M, const double* u,
     P[K::X * NDP] = VF == VF_KENNEDY_GRUBER ? 0.5 * s.beta : s.beta;
   }
   if constexpr (VF == VF_CHANDRASHEKAR) P[K::Y * NDP] = 0.5 * s.kin;
-  const int in = node % N, jn = (node / N) % N, kn = DIM == 3 ? node / (N * N) : 0;
-  double jdet = __ldg(M.tab.jdiag[0] + I[0] * N + in);
-  if (DIM == 2) {
-    jdet = jdet * __ldg(M.tab.jdiag[1] + I[1] * N + jn);
-  } else {
-    jdet = jdet * (__ldg(M.tab.jdiag[1] + I[1] * N + jn) * __ldg(M.tab.jdiag[2] + I[2] * N + kn));
+  if (mij_pre) {  // element_tables_kernel computed it with the expression below
+    P[K::MIJ * NDP] = *mij_pre;
+    return;
   }
-  P[K::MIJ * NDP] = -(1.0 / jdet);
+  const int in = node % N, jn = (node / N) % N, kn = DIM == 3 ? node / (N * N) : 0;
+  P[K::MIJ * NDP] = node_minus_inv_j<DIM, N>(M.tab, I[0], I[1], I[2], in, jn, kn);
 }
 
 // Surface lifting of one node (surface_integral.hpp:35-154): per direction,
@@ -544,6 +579,11 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile 
   const double* tile_src = M.u_in + (int64_t)e0 * NV * ND;
   ElementTileLoad<N, NV, ND, NDP, EPB, NT> tload;
   if (worker) tload.issue(tile_src, ne, tid);
+  // -1/J of this thread's node from the mesh's table, requested with the tile
+  const int el = tid / ND, node = tid % ND;
+  const bool active = el < ne;
+  double mij_node = 0.0;
+  if (M.mij && active) mij_node = __ldg(M.mij + (int64_t)(e0 + el) * ND + node);
   __shared__ uint64_t bar_n;
   bool bulk_n = false;
   if constexpr (S::SM_N > 0 && !PERSIST)
@@ -555,7 +595,11 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile 
     mbar_arrive_expect_tx(&bar_n, bytes);
     if (!p.skip_tile_copy) bulk_copy_g2s(stage_n, M.u_n + (int64_t)e0 * NV * ND, bytes, &bar_n);
   }
-  node_element_info<DIM, NI>(M, info, e0, ne, tid, NT);
+  if (M.info) {
+    for (int k = tid; k < ne * NI; k += NT) info[k] = __ldg(M.info + (int64_t)e0 * NI + k);
+  } else {
+    node_element_info<DIM, NI>(M, info, e0, ne, tid, NT);
+  }
   if constexpr (HG) {
     for (int k = tid; k < N * N; k += NT) vinv_s[k] = p.basis.Vinv[k / N][k % N];
   }
@@ -563,14 +607,13 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile 
   __syncthreads();
 
   // ---- phase 1: node data, squared sound speed and -1/J ------------------
-  const int el = tid / ND, node = tid % ND;
-  const bool active = el < ne;
   const int pn = padn<N, S::PAD>(node);
   if (active) {
     double u[NV];
 #pragma unroll
     for (int q = 0; q < NV; ++q) u[q] = us[(el * NV + q) * NDP + pn];
-    node_prepare<DIM, N, VF, NDP>(M, u, gamma, info + el * NI, node, pr + el * NQ * NDP + pn);
+    node_prepare<DIM, N, VF, NDP>(M, u, gamma, info + el * NI, node, pr + el * NQ * NDP + pn,
+                                  M.mij ? &mij_node : nullptr);
     if constexpr (NS && DIM == 3) {
       // -F_v at the node from the lifted gradient (parabolic_viscous.hpp:358-396)
       double q[5], g[3][4];

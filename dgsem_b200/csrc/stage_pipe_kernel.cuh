@@ -97,7 +97,15 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
     const bool active = el < ne;
 
     // ---- element info ------------------------------------------------------
-    node_element_info<DIM, NI>(M, info, e0, ne, tid, NT);
+    if (M.info) {
+      for (int k = tid; k < ne * NI; k += NT) info[k] = __ldg(M.info + (int64_t)e0 * NI + k);
+    } else {
+      node_element_info<DIM, NI>(M, info, e0, ne, tid, NT);
+    }
+    // -1/J of this thread's node from the mesh's table, requested before
+    // the wait for the tile
+    double mij_node = 0.0;
+    if (M.mij && active) mij_node = __ldg(M.mij + (int64_t)(e0 + el) * ND + node);
     // the block agrees on a timeout (vote) so that all of it leaves together
     if (__syncthreads_or(!mbar_wait_bounded(&bar_in, phase, p.wait_limit_ns))) {
       if (tid == 0) atomicOr(p.nonfinite, 2u);
@@ -112,7 +120,8 @@ __device__ __forceinline__ void stage_pipe_body(const StageArgs<N>& p, int ntile
         u[q] = stage_in[(el * NV + q) * ND + node];
         us[(el * NV + q) * NDP + pn] = u[q];
       }
-      node_prepare<DIM, N, VF, NDP>(M, u, gamma, info + el * NI, node, pr + el * NQ * NDP + pn);
+      node_prepare<DIM, N, VF, NDP>(M, u, gamma, info + el * NI, node, pr + el * NQ * NDP + pn,
+                                    M.mij ? &mij_node : nullptr);
     }
     __syncthreads();
     // stage_in is consumed: request the next tile's u_in
