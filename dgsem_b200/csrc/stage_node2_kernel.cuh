@@ -154,20 +154,30 @@ __device__ __forceinline__ void stage_node2_body(const StageArgs<N>& p) {
   const double t_stage = p.t_dev ? (*p.t_dev + p.t) : p.t;
   const int c0 = M.cells[0], c1 = M.cells[1], c2 = M.cells[2];
 
-  // ---- phase 0: the u_in tile, the epilogue's u_n tile, element info ----
-  // (issue order as in stage_node_body: u_in loads, the u_n bulk copy, the
-  // element info while the loads are in flight, then the tile store)
-  const double* tile_src = M.u_in + (int64_t)e0 * NV * ND;
-  ElementTileLoad<N, NV, ND, NDP, EPB, NT> tload;
-  tload.issue(tile_src, ne, tid);
+  // ---- phases 0 and 1: the u_in tile, the u_n tile, element info, node
+  // data (as in stage_node_body: with the mesh's tables every thread reads
+  // its own two nodes and computes their data before the one barrier) -----
   const int el = tid / NH, h = tid % NH;
   const int nA = h, nB = h + NH;
   const bool active = el < ne;
-  // -1/J of the two nodes from the mesh's table, requested with the tile
+  const bool own_node = M.mij != nullptr && M.info != nullptr;
+  const double* tile_src = M.u_in + (int64_t)e0 * NV * ND;
+  ElementTileLoad<N, NV, ND, NDP, EPB, NT> tload;
+  double u2[2][NV];
   double mij_ab[2] = {0.0, 0.0};
-  if (M.mij && active) {
-    mij_ab[0] = __ldg(M.mij + (int64_t)(e0 + el) * ND + nA);
-    mij_ab[1] = __ldg(M.mij + (int64_t)(e0 + el) * ND + nB);
+  if (own_node) {
+    if (active) {
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        const int node = s ? nB : nA;
+#pragma unroll
+        for (int q = 0; q < NV; ++q)
+          u2[s][q] = __ldg(M.u_in + ((int64_t)(e0 + el) * NV + q) * ND + node);
+        mij_ab[s] = __ldg(M.mij + (int64_t)(e0 + el) * ND + node);
+      }
+    }
+  } else {
+    tload.issue(tile_src, ne, tid);
   }
   __shared__ uint64_t bar_n;
   bool bulk_n = false;
@@ -185,19 +195,23 @@ __device__ __forceinline__ void stage_node2_body(const StageArgs<N>& p) {
   } else {
     node_element_info<DIM, NI>(M, info, e0, ne, tid, NT);
   }
-  tload.store(tile_src, us, ne, tid);
-  __syncthreads();
-
-  // ---- phase 1: node data of both nodes ----------------------------------
+  if (!own_node) {
+    tload.store(tile_src, us, ne, tid);
+    __syncthreads();
+  }
   if (active) {
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
       const int node = s ? nB : nA;
-      double u[NV];
+      if (own_node) {
 #pragma unroll
-      for (int q = 0; q < NV; ++q) u[q] = us[(el * NV + q) * NDP + node];
-      node_prepare<DIM, N, VF, NDP>(M, u, gamma, info + el * NI, node, pr + el * NQ * NDP + node,
-                                    M.mij ? &mij_ab[s] : nullptr);
+        for (int q = 0; q < NV; ++q) us[(el * NV + q) * NDP + node] = u2[s][q];
+      } else {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) u2[s][q] = us[(el * NV + q) * NDP + node];
+      }
+      node_prepare<DIM, N, VF, NDP>(M, u2[s], gamma, info + el * NI, node,
+                                    pr + el * NQ * NDP + node, own_node ? &mij_ab[s] : nullptr);
     }
   }
   __syncthreads();

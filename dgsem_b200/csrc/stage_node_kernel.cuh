@@ -571,19 +571,33 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile 
   const double t_stage = p.t_dev ? (*p.t_dev + p.t) : p.t;
   const int c0 = M.cells[0], c1 = M.cells[1], c2 = M.cells[2];
 
-  // ---- phase 0: the u_in tile, the epilogue's u_n tile, element info ----
-  // The u_in loads are issued first; the u_n tile is requested as one bulk
-  // copy that arrives while the block computes (block-uniform decision); the
-  // element info is computed while the u_in loads are in flight, then the
-  // tile is stored to shared memory.
-  const double* tile_src = M.u_in + (int64_t)e0 * NV * ND;
-  ElementTileLoad<N, NV, ND, NDP, EPB, NT> tload;
-  if (worker) tload.issue(tile_src, ne, tid);
-  // -1/J of this thread's node from the mesh's table, requested with the tile
+  // ---- phases 0 and 1: the u_in tile, the epilogue's u_n tile, element
+  // info, node data ----------------------------------------------------------
+  // With the mesh's tables (single-mesh launches: -1/J and the element info
+  // precomputed) every thread reads its own node's state, coalesced per
+  // variable, and computes its node data without waiting for the rest of the
+  // tile: one barrier for both phases.  Otherwise the tile's loads are issued
+  // first, the element info is computed while they are in flight, and the
+  // node data follow a barrier.  Either way the u_n tile is requested as one
+  // bulk copy that arrives while the block computes (block-uniform decision).
   const int el = tid / ND, node = tid % ND;
   const bool active = el < ne;
+  const int pn = padn<N, S::PAD>(node);
+  const bool own_node = M.mij != nullptr && M.info != nullptr;
+  const double* tile_src = M.u_in + (int64_t)e0 * NV * ND;
+  ElementTileLoad<N, NV, ND, NDP, EPB, NT> tload;
+  double u[NV];
   double mij_node = 0.0;
-  if (M.mij && active) mij_node = __ldg(M.mij + (int64_t)(e0 + el) * ND + node);
+  if (own_node) {
+    if (active) {
+#pragma unroll
+      for (int q = 0; q < NV; ++q)
+        u[q] = __ldg(M.u_in + ((int64_t)(e0 + el) * NV + q) * ND + node);
+      mij_node = __ldg(M.mij + (int64_t)(e0 + el) * ND + node);
+    }
+  } else if (worker) {
+    tload.issue(tile_src, ne, tid);
+  }
   __shared__ uint64_t bar_n;
   bool bulk_n = false;
   if constexpr (S::SM_N > 0 && !PERSIST)
@@ -603,17 +617,10 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile 
   if constexpr (HG) {
     for (int k = tid; k < N * N; k += NT) vinv_s[k] = p.basis.Vinv[k / N][k % N];
   }
-  if (worker) tload.store(tile_src, us, ne, tid);
-  __syncthreads();
-
-  // ---- phase 1: node data, squared sound speed and -1/J ------------------
-  const int pn = padn<N, S::PAD>(node);
-  if (active) {
-    double u[NV];
-#pragma unroll
-    for (int q = 0; q < NV; ++q) u[q] = us[(el * NV + q) * NDP + pn];
+  // node data, squared sound speed and -1/J (and -F_v with viscous terms)
+  auto node_data = [&](const double* u) {
     node_prepare<DIM, N, VF, NDP>(M, u, gamma, info + el * NI, node, pr + el * NQ * NDP + pn,
-                                  M.mij ? &mij_node : nullptr);
+                                  own_node ? &mij_node : nullptr);
     if constexpr (NS && DIM == 3) {
       // -F_v at the node from the lifted gradient (parabolic_viscous.hpp:358-396)
       double q[5], g[3][4];
@@ -647,6 +654,21 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile 
 #pragma unroll
         for (int v = 0; v < 4; ++v) wv[((el * 2 + d) * NV + v) * ND + node] = f[v];
       }
+    }
+  };
+  if (own_node) {
+    if (active) {
+#pragma unroll
+      for (int q = 0; q < NV; ++q) us[(el * NV + q) * NDP + pn] = u[q];
+      node_data(u);
+    }
+  } else {
+    if (worker) tload.store(tile_src, us, ne, tid);
+    __syncthreads();
+    if (active) {
+#pragma unroll
+      for (int q = 0; q < NV; ++q) u[q] = us[(el * NV + q) * NDP + pn];
+      node_data(u);
     }
   }
   __syncthreads();
