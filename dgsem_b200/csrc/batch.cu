@@ -49,6 +49,9 @@ struct dgsem_batch {
   std::vector<int64_t> nelem;
   std::vector<int> nodes;
   std::vector<DeviceTables> tabs;
+  // per-mesh element info and -1/J tables of the node-parallel kernels
+  std::vector<const int*> minfo;
+  std::vector<const double*> mmij;
   std::vector<Group> groups;
   cudaStream_t stream = nullptr;
   cudaEvent_t fork = nullptr;
@@ -130,6 +133,8 @@ dgsem_status upload_views(dgsem_batch* b, double* u, const double* dt) {
       }
       v.nelem = (int)b->nelem[m];
       v.tab = b->tabs[m];
+      v.info = b->minfo[m];
+      v.mij = b->mmij[m];
     }
   cudaError_t e = cudaMemcpyAsync(b->views, b->views_host.data(),
                                   b->views_host.size() * sizeof(MeshView),
@@ -423,7 +428,7 @@ dgsem_status dgsem_batch_create(const dgsem_mesh_desc* meshes, int n_meshes,
     c.basis = bases[g.n];
     c.nonfinite = b->flag;
     c.grad = nullptr;
-    c.elem_info = nullptr;  // batched launches compute the element info in the kernel
+    c.elem_info = nullptr;  // batched launches take the tables from the mesh views
     c.mij = nullptr;
     for (int f = 0; f < 6; ++f) c.bc.kind[f] = 0;
     g.members = kv.second;
@@ -443,6 +448,39 @@ dgsem_status dgsem_batch_create(const dgsem_mesh_desc* meshes, int n_meshes,
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming);
     b->groups.push_back(std::move(g));
+  }
+  // per-mesh element info and -1/J tables, built by the mesh's degree engine
+  if (e == cudaSuccess) {
+    int64_t nel_total = 0, nodes_total = 0;
+    for (int m = 0; m < n_meshes; ++m) {
+      nel_total += b->nelem[m];
+      nodes_total += b->nelem[m] * b->nodes[m];
+    }
+    int* info = balloc<int>(b, (size_t)nel_total * 12);
+    double* mij = info ? balloc<double>(b, (size_t)nodes_total) : nullptr;
+    if (!mij) {
+      bfree(b);
+      delete b;
+      return DGSEM_ERR_ALLOC;
+    }
+    b->minfo.assign(n_meshes, nullptr);
+    b->mmij.assign(n_meshes, nullptr);
+    int64_t io = 0, mo = 0;
+    for (const Group& g : b->groups)
+      for (int m : g.members) {
+        MeshView v{};
+        for (int a = 0; a < 3; ++a) {
+          v.cells[a] = a < nd ? (int)meshes[m].n_cells[a] : 1;
+          v.periodic[a] = 1;
+        }
+        v.nelem = (int)b->nelem[m];
+        v.tab = b->tabs[m];
+        if (e == cudaSuccess) e = g.engine->build_mesh_tables(v, info + io, mij + mo, nullptr);
+        b->minfo[m] = info + io;
+        b->mmij[m] = mij + mo;
+        io += b->nelem[m] * 12;
+        mo += b->nelem[m] * b->nodes[m];
+      }
   }
   if (e == cudaSuccess) e = build_persistent(b);
   if (e == cudaSuccess) e = cudaDeviceSynchronize();

@@ -404,7 +404,16 @@ dgsem_status dgsem_ctx_create(const dgsem_mesh_desc* mesh,
   }
   cudaMemset(ctx->flag, 0, sizeof(unsigned int));
   c.nonfinite = ctx->flag;
-  err = ctx->engine->build_mesh_tables(c, info_tab, mij_tab, nullptr);
+  {
+    MeshView mv{};
+    for (int i = 0; i < 3; ++i) {
+      mv.cells[i] = (int)c.cells[i];
+      mv.periodic[i] = c.periodic[i];
+    }
+    mv.nelem = (int)c.nelem;
+    mv.tab = c.tab;
+    err = ctx->engine->build_mesh_tables(mv, info_tab, mij_tab, nullptr);
+  }
   if (err == cudaSuccess) {
     c.elem_info = info_tab;
     c.mij = mij_tab;

@@ -68,8 +68,10 @@ class EngineBase {
   // number of diag slots (blocks) the last stage launch with diag wrote
   virtual int64_t last_diag_slots() const = 0;
   // Fills the per-mesh tables of the node-parallel kernels (EngineConfig::
-  // elem_info, 12 ints per element; ::mij, -1/J per node) on stream s.
-  virtual cudaError_t build_mesh_tables(const EngineConfig& cfg, int* info, double* mij,
+  // elem_info / MeshView::info, 12 ints per element; ::mij, -1/J per node)
+  // of the mesh `m` (its cells, periodicity, element count and metric
+  // tables) on stream s.
+  virtual cudaError_t build_mesh_tables(const MeshView& m, int* info, double* mij,
                                         cudaStream_t s) const = 0;
   // Batched launch over a tile list (mesh index and first element per block)
   // of meshes sharing this engine's scheme and degree; per-mesh data in
@@ -433,16 +435,9 @@ class Engine final : public EngineBase {
     }
   }
 
-  cudaError_t build_mesh_tables(const EngineConfig& cfg, int* info, double* mij,
+  cudaError_t build_mesh_tables(const MeshView& m, int* info, double* mij,
                                 cudaStream_t s) const override {
-    MeshView m{};
-    for (int i = 0; i < 3; ++i) {
-      m.cells[i] = (int)cfg.cells[i];
-      m.periodic[i] = cfg.periodic[i];
-    }
-    m.nelem = (int)cfg.nelem;
-    m.tab = cfg.tab;
-    const int64_t nodes = cfg.nelem * ipow(N, DIM);
+    const int64_t nodes = (int64_t)m.nelem * ipow(N, DIM);
     const unsigned blocks = (unsigned)std::min<int64_t>((nodes + 255) / 256, 4096);
     element_tables_kernel<DIM, N, 12><<<blocks, 256, 0, s>>>(m, info, mij);
     return cudaGetLastError();
