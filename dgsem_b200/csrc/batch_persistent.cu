@@ -16,6 +16,14 @@ namespace {
 
 constexpr int kThreads = 128;
 
+// Elements per work item of degree n: as many as fit in the 128 threads of
+// the persistent block (the per-degree launches may use wider blocks).
+template <int N>
+struct PersistLaunch {
+  static constexpr int EPB = 128 / (N * N) > 0 ? 128 / (N * N) : 1;
+  static constexpr int NT = EPB * N * N;
+};
+
 template <int VF, int SF>
 struct PersistArgs {
   StageArgs<2> a2;
@@ -31,7 +39,7 @@ struct PersistArgs {
 
 template <int N, int VF, int SF>
 __device__ __forceinline__ void run_item(const StageArgs<N>& a, int tile) {
-  using NL = NodeLaunch<2, N>;
+  using NL = PersistLaunch<N>;
   static_assert(NL::NT <= kThreads, "tile wider than the persistent block");
   stage_node_body<2, N, VF, SF, NL::EPB, true, false, false, kThreads, true>(a, tile);
 }
@@ -61,7 +69,7 @@ __global__ void __launch_bounds__(kThreads, 5) batch_persistent_kernel(const Per
 
 template <int N>
 constexpr size_t smem_of(int vf) {
-  using NL = NodeLaunch<2, N>;
+  using NL = PersistLaunch<N>;
   return vf == VF_CHANDRASHEKAR ? NodeShape<2, N, VF_CHANDRASHEKAR, NL::EPB>::smem_bytes_base
          : vf == VF_RANOCHA     ? NodeShape<2, N, VF_RANOCHA, NL::EPB>::smem_bytes_base
                                 : NodeShape<2, N, VF_KENNEDY_GRUBER, NL::EPB>::smem_bytes_base;
@@ -126,13 +134,13 @@ bool persistent_supported(int ndims, int vf, int sf) {
 
 int persistent_elements_per_tile(int n) {
   switch (n) {
-    case 2: return NodeLaunch<2, 2>::EPB;
-    case 3: return NodeLaunch<2, 3>::EPB;
-    case 4: return NodeLaunch<2, 4>::EPB;
-    case 5: return NodeLaunch<2, 5>::EPB;
-    case 6: return NodeLaunch<2, 6>::EPB;
-    case 7: return NodeLaunch<2, 7>::EPB;
-    default: return NodeLaunch<2, 8>::EPB;
+    case 2: return PersistLaunch<2>::EPB;
+    case 3: return PersistLaunch<3>::EPB;
+    case 4: return PersistLaunch<4>::EPB;
+    case 5: return PersistLaunch<5>::EPB;
+    case 6: return PersistLaunch<6>::EPB;
+    case 7: return PersistLaunch<7>::EPB;
+    default: return PersistLaunch<8>::EPB;
   }
 }
 

@@ -157,13 +157,29 @@ struct LaunchShape {
   static constexpr int MINB = V == 1 ? (65536 / (NT * 100) > 1 ? 65536 / (NT * 100) : 2) : 0;
 };
 
-// Node-parallel variants: about 128 threads per block, one per node;
-// variant 3 caps registers at ~72 per thread (7 resident blocks of 128),
-// variant 4 leaves them to the compiler.
+// Fraction of the lanes of its warps that a block of `threads` threads uses.
+constexpr double lane_use(int threads) { return double(threads) / (((threads + 31) / 32) * 32); }
+
+// Elements per block of the node-parallel shapes: 128 / n^d (about 128
+// threads), unless that leaves more than 5 % of the block's warp lanes idle
+// (n^d = 36, 49 in 2D; 27 in 3D); then the smallest count up to 256 threads
+// that fills at least 95 % of them (a partly filled warp costs a whole
+// warp's issue slots).
+constexpr int node_elements_per_block(int nd) {
+  const int e0 = 128 / nd > 0 ? 128 / nd : 1;
+  if (lane_use(e0 * nd) >= 0.95) return e0;
+  for (int e = e0 + 1; e * nd <= 256; ++e)
+    if (lane_use(e * nd) >= 0.95) return e;
+  return e0;
+}
+
+// Node-parallel variants: one thread per node; variant 3 caps registers at
+// ~72 per thread (7 resident blocks of 128 threads), variant 4 leaves them to
+// the compiler.
 template <int DIM, int N>
 struct NodeLaunch {
   static constexpr int ND = ipow(N, DIM);
-  static constexpr int EPB = (128 / ND) > 0 ? (128 / ND) : 1;
+  static constexpr int EPB = node_elements_per_block(ND);
   static constexpr int NT = EPB * ND;
   static constexpr int MINB = 65536 / (NT * 72) > 1 ? 65536 / (NT * 72) : 1;
 };

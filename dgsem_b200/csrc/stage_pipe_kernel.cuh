@@ -36,9 +36,11 @@ struct PipeShape {
       sizeof(int) * EPB * NI;
   static constexpr bool kSupported = (NV * ND) % 2 == 0;
   // resident blocks per SM allowed by shared memory (228 KB, 1 KB reserved
-  // per block), capped at 7 (72 registers per thread at 128 threads)
+  // per block), capped at 72 registers per thread (7 blocks of 128 threads)
   static constexpr int MINB_SMEM = int((228 * 1024) / (smem_bytes + 1024));
-  static constexpr int MINB = MINB_SMEM < 7 ? (MINB_SMEM > 0 ? MINB_SMEM : 1) : 7;
+  static constexpr int MINB_REG = 65536 / (NT * 72) > 1 ? 65536 / (NT * 72) : 1;
+  static constexpr int MINB_CAP = MINB_SMEM < MINB_REG ? MINB_SMEM : MINB_REG;
+  static constexpr int MINB = MINB_CAP > 0 ? MINB_CAP : 1;
 };
 
 template <int DIM, int N, int VF, int SF, int EPB>
