@@ -89,6 +89,17 @@ struct MeshView {
   const double* mij;
 };
 
+// Copies the view of mesh m into shared memory, one 8-byte word per thread
+// (the block's first sizeof(MeshView) / 8 threads); the caller synchronises.
+__device__ __forceinline__ void copy_mesh_view(MeshView* dst, const MeshView* meshes, int m,
+                                               int tid) {
+  static_assert(sizeof(MeshView) % 8 == 0, "mesh view words");
+  constexpr int MW = int(sizeof(MeshView) / 8);
+  if (tid < MW)
+    reinterpret_cast<unsigned long long*>(dst)[tid] =
+        __ldg(reinterpret_cast<const unsigned long long*>(meshes + m) + tid);
+}
+
 template <int N>
 struct StageArgs {
   MeshView mesh;           // single-mesh launches
@@ -924,20 +935,23 @@ __device__ __forceinline__ void stage_body(const StageArgs<N>& p) {
   double* vinv_s = wv + S::SM_W;     // inverse Legendre Vandermonde (HG)
   int* info = reinterpret_cast<int*>(vinv_s + S::SM_VINV);
 
-  stage_dependency_sync();
   const int tid = threadIdx.x;
   // Batched launches stage the block's mesh view in shared memory; single-mesh
   // launches read it from the kernel parameters (constant bank), which keeps
-  // the table pointers out of shared-memory loads in the line loop.
+  // the table pointers out of shared-memory loads in the line loop.  The tile
+  // list and the mesh views are written by host copies only, so they are
+  // read before waiting for the previous kernel.
   __shared__ MeshView mesh_s;
   int e0;
   if constexpr (BATCH) {
+    static_assert(NT >= int(sizeof(MeshView) / 8), "block narrower than the mesh view");
     e0 = p.tile_e0[blockIdx.x];
-    if (tid == 0) mesh_s = p.meshes[p.tile_mesh[blockIdx.x]];
-    __syncthreads();
+    copy_mesh_view(&mesh_s, p.meshes, p.tile_mesh[blockIdx.x], tid);
   } else {
     e0 = (int)blockIdx.x * EPB;
   }
+  stage_dependency_sync();
+  if constexpr (BATCH) __syncthreads();
   const MeshView& M = BATCH ? mesh_s : p.mesh;
   const int nelem = M.nelem;
   if (e0 >= nelem) return;

@@ -549,20 +549,24 @@ __device__ __forceinline__ void stage_node_body(const StageArgs<N>& p, int tile 
   // [el][var][node] u_n tile (bulk-copy target; present when p.a != 0)
   double* stage_n = reinterpret_cast<double*>(reinterpret_cast<char*>(smem_node) + S::off_n_bytes);
 
-  stage_dependency_sync();
   const int tid = threadIdx.x;
   __shared__ MeshView mesh_s;
   int e0;
   // threads past the element tile (wider persistent blocks) only join barriers
   const bool worker = NTB == 0 || tid < NT;
+  // the tile list and the mesh views are written by host copies only, so
+  // they are read before waiting for the previous kernel
   if constexpr (BATCH) {
+    static_assert((NTB > 0 ? NTB : NT) >= int(sizeof(MeshView) / 8),
+                  "block narrower than the mesh view");
     const int tl = PERSIST ? tile : (int)blockIdx.x;
     e0 = p.tile_e0[tl];
-    if (tid == 0) mesh_s = p.meshes[p.tile_mesh[tl]];
-    __syncthreads();
+    copy_mesh_view(&mesh_s, p.meshes, p.tile_mesh[tl], tid);
   } else {
     e0 = (int)blockIdx.x * EPB;
   }
+  stage_dependency_sync();
+  if constexpr (BATCH) __syncthreads();
   const MeshView& M = BATCH ? mesh_s : p.mesh;
   const int nelem = M.nelem;
   if (e0 >= nelem) return;

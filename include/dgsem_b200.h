@@ -258,10 +258,10 @@ dgsem_status dgsem_batch_autotune(dgsem_batch* b, double* u, const double* dt_ho
                                   int* chosen);
 dgsem_status dgsem_batch_launch_count(const dgsem_batch* b, int64_t* count);
 /* Persistent mode (2D batches, LLF surface flux): every stage is ONE launch
- * over the meshes of all degrees; each block of 128 threads walks a work list
+ * over the meshes of all degrees; each block of 256 threads walks a work list
  * of (degree, element tile) items, higher degrees first, and runs that
  * degree's node-parallel stage body.  Results agree with the per-degree
- * launches to rounding (the same body and tiles; bit for bit where the
+ * launches to rounding (the same stage body; bit for bit where the
  * compiler emits the same arithmetic).  DGSEM_ERR_UNSUPPORTED for other
  * batches.  Graphs record the mode they were captured in. */
 /* Selects one launch shape (dgsem_set_launch_variant's numbering) for every
