@@ -61,7 +61,7 @@ __device__ __forceinline__ double adj_inv_j(const DeviceTables& t, int ie, int j
   return 1.0 / (__ldg(t.jdiag[0] + ie * N + node % N) * __ldg(t.jdiag[1] + je * N + node / N));
 }
 
-// ---- derivatives of the logarithmic mean (same branch rule as ln_mean_parts)
+// ---- derivatives of the logarithmic mean (same branch rule as chandrashekar_means)
 // mean(x, y) and d mean / dx
 __device__ __forceinline__ void ln_mean_dx(double x, double y, double& m, double& dm) {
   const double s = x + y;

@@ -31,25 +31,37 @@ struct NodeState {
   double inv_rho;
 };
 
-// Logarithmic mean and its inverse with the reference's branch rule
-// (series when f^2 < 1e-4, else (y-x)/log(y/x)).  The series branch reuses one
-// reciprocal of x+y for f^2 and for the inverse mean.
-__device__ __forceinline__ void ln_mean_parts(double x, double y, double& mean,
-                                              double& inv_mean) {
-  const double s = x + y;
-  const double r = 1.0 / s;
-  const double t = (x - y) * r;
+// The means of Chandrashekar's flux for one pair (numerical_flux.hpp:436-500):
+// the logarithmic mean of rho, the inverse logarithmic mean of beta and
+// 1 / (beta_L + beta_R), with the reference's branch rule for each logarithmic
+// mean (series when f^2 = ((x-y)/(x+y))^2 < 1e-4, else (y-x)/log(y/x)).
+// Series branches: the mean is (x+y)/2 / (1 + f^2/3 + f^4/5 + f^6/7), taken as
+// (x+y)/2 times the reciprocal series 1 - f^2/3 - 4 f^4/45 - 44 f^6/945 (the
+// next term, 1147 f^8/14175, is below 1e-17 relative for f^2 < 1e-4), and the
+// inverse mean reuses 1/(x+y); so the pair needs two divisions, 1/(rho sum)
+// and 1/(beta sum), instead of four.
+__device__ __forceinline__ void chandrashekar_means(double rL, double rR, double bL, double bR,
+                                                    double& rho_mean, double& inv_beta_mean,
+                                                    double& inv_beta_sum) {
+  const double s = rL + rR;
+  const double t = (rL - rR) / s;
   const double f2 = t * t;
   if (f2 < 1.0e-4) {
-    const double poly =
-        2.0 + f2 * (2.0 / 3.0 + f2 * (2.0 / 5.0 + f2 * (2.0 / 7.0)));
-    mean = s / poly;
-    inv_mean = poly * r;
+    rho_mean = (0.5 * s) * (1.0 + f2 * (-1.0 / 3.0 + f2 * (-4.0 / 45.0 + f2 * (-44.0 / 945.0))));
   } else {
-    const double lg = log(y / x);
-    mean = (y - x) / lg;
-    inv_mean = lg / (y - x);
+    rho_mean = (rR - rL) / log(rR / rL);
   }
+  const double sb = bL + bR;
+  const double rb = 1.0 / sb;
+  const double tb = (bL - bR) * rb;
+  const double g2 = tb * tb;
+  if (g2 < 1.0e-4) {
+    inv_beta_mean = (2.0 + g2 * (2.0 / 3.0 + g2 * (2.0 / 5.0 + g2 * (2.0 / 7.0)))) * rb;
+  } else {
+    const double lg = log(bR / bL);
+    inv_beta_mean = lg / (bR - bL);
+  }
+  inv_beta_sum = rb;
 }
 
 __device__ __forceinline__ double ln_mean(double x, double y) {
@@ -116,11 +128,9 @@ __device__ __forceinline__ void volume_flux(const NodeState<DIM>& L,
   if (VF == VF_CHANDRASHEKAR) {
     // numerical_flux.hpp:436-500: rho_mean = ln(rho), beta_mean = ln(beta),
     // p_mean = 0.5 rho_avg / beta_avg = 0.5 (rhoL+rhoR) / (betaL+betaR).
-    double rho_mean, unused;
-    ln_mean_parts(L.rho, R.rho, rho_mean, unused);
-    double beta_mean_unused, inv_beta_mean;
-    ln_mean_parts(L.beta, R.beta, beta_mean_unused, inv_beta_mean);
-    const double p_mean = 0.5 * (L.rho + R.rho) / (L.beta + R.beta);
+    double rho_mean, inv_beta_mean, inv_beta_sum;
+    chandrashekar_means(L.rho, R.rho, L.beta, R.beta, rho_mean, inv_beta_mean, inv_beta_sum);
+    const double p_mean = 0.5 * (L.rho + R.rho) * inv_beta_sum;
     const double f1 = rho_mean * 0.5 * (vnL + vnR);
     f[0] = f1;
     double fe = f1 * 0.5 * (inv_gm1 * inv_beta_mean - (L.kin + R.kin));

@@ -160,10 +160,9 @@ __device__ __forceinline__ void node_volume_flux(const NodeFluxState<DIM>& L,
       hvnL += L.v[d] * n[d];
       hvnR += R.v[d] * n[d];
     }
-    double rho_mean, unused, beta_mean_unused, inv_beta_mean;
-    ln_mean_parts(L.rho, R.rho, rho_mean, unused);
-    ln_mean_parts(L.x, R.x, beta_mean_unused, inv_beta_mean);
-    const double p_mean = (L.hrho + R.hrho) / (L.x + R.x);
+    double rho_mean, inv_beta_mean, inv_beta_sum;
+    chandrashekar_means(L.rho, R.rho, L.x, R.x, rho_mean, inv_beta_mean, inv_beta_sum);
+    const double p_mean = (L.hrho + R.hrho) * inv_beta_sum;
     const double f1 = rho_mean * (hvnL + hvnR);
     f[0] = f1;
     double fe = f1 * (hgm1 * inv_beta_mean - (L.y + R.y));
