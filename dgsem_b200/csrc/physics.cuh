@@ -64,15 +64,14 @@ __device__ __forceinline__ void chandrashekar_means(double rL, double rR, double
   inv_beta_sum = rb;
 }
 
+// Logarithmic mean with the reference's branch rule; the series branch as in
+// chandrashekar_means (one division).
 __device__ __forceinline__ double ln_mean(double x, double y) {
   const double s = x + y;
   const double t = (x - y) / s;
   const double f2 = t * t;
-  if (f2 < 1.0e-4) {
-    const double poly =
-        2.0 + f2 * (2.0 / 3.0 + f2 * (2.0 / 5.0 + f2 * (2.0 / 7.0)));
-    return s / poly;
-  }
+  if (f2 < 1.0e-4)
+    return (0.5 * s) * (1.0 + f2 * (-1.0 / 3.0 + f2 * (-4.0 / 45.0 + f2 * (-44.0 / 945.0))));
   return (y - x) / log(y / x);
 }
 
