@@ -4,7 +4,7 @@
 // Every flux works on per-node primitive data prepared once per node
 // (`NodeState`), so the per-pair cost is only the two-point averages.  The
 // formulas follow the reference's plugins:
-//   ln_mean                      base/math_utils.hpp:8-25
+//   ln_mean (ln_mean_rs)         base/math_utils.hpp:8-25
 //   ChandrashekarFlux 2D/3D      base/numerical_flux.hpp:436-500, 520-594
 //   LaxFriedrichsFlux 2D/3D      base/numerical_flux.hpp:198-228, 39-69
 //   LLF wave speed |v.n|+a|n|    equations/compressible_euler2D.hpp:70-109
@@ -31,6 +31,33 @@ struct NodeState {
   double inv_rho;
 };
 
+// Reciprocals of two positive sums with one division, 1/(a b) times the
+// other factor.  The sums are of densities, pressures, rho p products or
+// rho / p ratios of one pair of nodes, far inside the normal range, so a b
+// neither overflows nor underflows.
+__device__ __forceinline__ void two_reciprocals(double a, double b, double& ra, double& rb) {
+  const double r = 1.0 / (a * b);
+  ra = r * b;
+  rb = r * a;
+}
+
+// The logarithmic mean (series branch: (x+y)/2 times the reciprocal series
+// of chandrashekar_means) and the inverse logarithmic mean, each given the
+// reciprocal rs of s = x + y; the reference's branch rule.
+__device__ __forceinline__ double ln_mean_rs(double x, double y, double s, double rs) {
+  const double t = (x - y) * rs;
+  const double f2 = t * t;
+  if (f2 < 1.0e-4)
+    return (0.5 * s) * (1.0 + f2 * (-1.0 / 3.0 + f2 * (-4.0 / 45.0 + f2 * (-44.0 / 945.0))));
+  return (y - x) / log(y / x);
+}
+__device__ __forceinline__ double inv_ln_mean_rs(double x, double y, double rs) {
+  const double t = (x - y) * rs;
+  const double f2 = t * t;
+  if (f2 < 1.0e-4) return (2.0 + f2 * (2.0 / 3.0 + f2 * (2.0 / 5.0 + f2 * (2.0 / 7.0)))) * rs;
+  return log(y / x) / (y - x);
+}
+
 // The means of Chandrashekar's flux for one pair (numerical_flux.hpp:436-500):
 // the logarithmic mean of rho, the inverse logarithmic mean of beta and
 // 1 / (beta_L + beta_R), with the reference's branch rule for each logarithmic
@@ -38,54 +65,18 @@ struct NodeState {
 // Series branches: the mean is (x+y)/2 / (1 + f^2/3 + f^4/5 + f^6/7), taken as
 // (x+y)/2 times the reciprocal series 1 - f^2/3 - 4 f^4/45 - 44 f^6/945 (the
 // next term, 1147 f^8/14175, is below 1e-17 relative for f^2 < 1e-4), and the
-// inverse mean reuses 1/(x+y); so the pair needs two divisions, 1/(rho sum)
-// and 1/(beta sum), instead of four.
+// inverse mean multiplies by 1/(x+y); the reciprocals of the rho and beta sums
+// come from one division, so the series branches of a pair need one division
+// instead of four.
 __device__ __forceinline__ void chandrashekar_means(double rL, double rR, double bL, double bR,
                                                     double& rho_mean, double& inv_beta_mean,
                                                     double& inv_beta_sum) {
-  const double s = rL + rR;
-  const double t = (rL - rR) / s;
-  const double f2 = t * t;
-  if (f2 < 1.0e-4) {
-    rho_mean = (0.5 * s) * (1.0 + f2 * (-1.0 / 3.0 + f2 * (-4.0 / 45.0 + f2 * (-44.0 / 945.0))));
-  } else {
-    rho_mean = (rR - rL) / log(rR / rL);
-  }
-  const double sb = bL + bR;
-  const double rb = 1.0 / sb;
-  const double tb = (bL - bR) * rb;
-  const double g2 = tb * tb;
-  if (g2 < 1.0e-4) {
-    inv_beta_mean = (2.0 + g2 * (2.0 / 3.0 + g2 * (2.0 / 5.0 + g2 * (2.0 / 7.0)))) * rb;
-  } else {
-    const double lg = log(bR / bL);
-    inv_beta_mean = lg / (bR - bL);
-  }
+  const double s = rL + rR, sb = bL + bR;
+  double rs, rb;
+  two_reciprocals(s, sb, rs, rb);
+  rho_mean = ln_mean_rs(rL, rR, s, rs);
+  inv_beta_mean = inv_ln_mean_rs(bL, bR, rb);
   inv_beta_sum = rb;
-}
-
-// Logarithmic mean with the reference's branch rule; the series branch as in
-// chandrashekar_means (one division).
-__device__ __forceinline__ double ln_mean(double x, double y) {
-  const double s = x + y;
-  const double t = (x - y) / s;
-  const double f2 = t * t;
-  if (f2 < 1.0e-4)
-    return (0.5 * s) * (1.0 + f2 * (-1.0 / 3.0 + f2 * (-4.0 / 45.0 + f2 * (-44.0 / 945.0))));
-  return (y - x) / log(y / x);
-}
-
-__device__ __forceinline__ double inv_ln_mean(double x, double y) {
-  const double s = x + y;
-  const double r = 1.0 / s;
-  const double t = (x - y) * r;
-  const double f2 = t * t;
-  if (f2 < 1.0e-4) {
-    const double poly =
-        2.0 + f2 * (2.0 / 3.0 + f2 * (2.0 / 5.0 + f2 * (2.0 / 7.0)));
-    return poly * r;
-  }
-  return log(y / x) / (y - x);
 }
 
 // Node preparation from conserved variables (rho, m_1..m_DIM, E).
@@ -142,9 +133,13 @@ __device__ __forceinline__ void volume_flux(const NodeState<DIM>& L,
     }
     f[DIM + 1] = fe;
   } else if (VF == VF_RANOCHA) {
-    const double rho_mean = ln_mean(L.rho, R.rho);
-    const double inv_rho_p_mean =
-        L.p * R.p * inv_ln_mean(L.rho * R.p, R.rho * L.p);
+    // the reciprocals of the two sums of the logarithmic means from one division
+    const double s1 = L.rho + R.rho;
+    const double x2 = L.rho * R.p, y2 = R.rho * L.p, s2 = x2 + y2;
+    double r1, r2;
+    two_reciprocals(s1, s2, r1, r2);
+    const double rho_mean = ln_mean_rs(L.rho, R.rho, s1, r1);
+    const double inv_rho_p_mean = L.p * R.p * inv_ln_mean_rs(x2, y2, r2);
     const double p_avg = 0.5 * (L.p + R.p);
     double vLvR = 0.0;
 #pragma unroll
