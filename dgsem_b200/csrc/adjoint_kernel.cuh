@@ -61,41 +61,50 @@ __device__ __forceinline__ double adj_inv_j(const DeviceTables& t, int ie, int j
   return 1.0 / (__ldg(t.jdiag[0] + ie * N + node % N) * __ldg(t.jdiag[1] + je * N + node / N));
 }
 
-// ---- derivatives of the logarithmic mean (same branch rule as chandrashekar_means)
+// ---- derivatives of the logarithmic mean (same branch rule as chandrashekar_means);
+// rs = 1 / (x + y) is given.  Series branch: with P = 2 (1 + f^2/3 + f^4/5 +
+// f^6/7), 1/P is the reciprocal series of chandrashekar_means; the log
+// branch shares 1/x and 1/log(y/x) (or 1/(y-x)) between its quotients.
 // mean(x, y) and d mean / dx
-__device__ __forceinline__ void ln_mean_dx(double x, double y, double& m, double& dm) {
+__device__ __forceinline__ void ln_mean_dx(double x, double y, double rs, double& m,
+                                           double& dm) {
   const double s = x + y;
-  const double t = (x - y) / s;
+  const double t = (x - y) * rs;
   const double f2 = t * t;
   if (f2 < 1.0e-4) {
-    const double P = 2.0 + f2 * (2.0 / 3.0 + f2 * (2.0 / 5.0 + f2 * (2.0 / 7.0)));
+    const double iP =
+        0.5 * (1.0 + f2 * (-1.0 / 3.0 + f2 * (-4.0 / 45.0 + f2 * (-44.0 / 945.0))));
     const double dP = 2.0 / 3.0 + f2 * (4.0 / 5.0 + f2 * (6.0 / 7.0));
-    const double df2 = 4.0 * t * y / (s * s);
-    m = s / P;
-    dm = 1.0 / P - s * dP * df2 / (P * P);
+    const double df2 = 4.0 * t * y * rs * rs;
+    m = s * iP;
+    dm = iP - s * dP * df2 * iP * iP;
   } else {
+    double ix, ilg;
     const double lg = log(y / x);
-    m = (y - x) / lg;
-    dm = (-lg + (y - x) / x) / (lg * lg);
+    two_reciprocals(x, lg, ix, ilg);
+    m = (y - x) * ilg;
+    dm = (-lg + (y - x) * ix) * ilg * ilg;
   }
 }
 
 // 1 / mean(x, y) and its x-derivative
-__device__ __forceinline__ void inv_ln_mean_dx(double x, double y, double& im, double& dim) {
-  const double s = x + y;
-  const double t = (x - y) / s;
+__device__ __forceinline__ void inv_ln_mean_dx(double x, double y, double rs, double& im,
+                                               double& dim) {
+  const double t = (x - y) * rs;
   const double f2 = t * t;
   if (f2 < 1.0e-4) {
     const double P = 2.0 + f2 * (2.0 / 3.0 + f2 * (2.0 / 5.0 + f2 * (2.0 / 7.0)));
     const double dP = 2.0 / 3.0 + f2 * (4.0 / 5.0 + f2 * (6.0 / 7.0));
-    const double df2 = 4.0 * t * y / (s * s);
-    im = P / s;
-    dim = dP * df2 / s - P / (s * s);
+    const double df2 = 4.0 * t * y * rs * rs;
+    im = P * rs;
+    dim = dP * df2 * rs - P * rs * rs;
   } else {
     const double lg = log(y / x);
     const double d = y - x;
-    im = lg / d;
-    dim = (lg - d / x) / (d * d);
+    double ix, id;
+    two_reciprocals(x, d, ix, id);
+    im = lg * id;
+    dim = (lg - d * ix) * id * id;
   }
 }
 
@@ -110,11 +119,12 @@ __device__ __forceinline__ void ec_flux_vjp_left(const NodeState<2>& L, const No
                                                  double& bb, double& kb) {
   const double vnL = L.v[0] * n[0] + L.v[1] * n[1];
   const double vnR = R.v[0] * n[0] + R.v[1] * n[1];
-  double rho_m, drho_m, ib, dib;
-  ln_mean_dx(L.rho, R.rho, rho_m, drho_m);
-  inv_ln_mean_dx(L.beta, R.beta, ib, dib);
-  const double bsum = L.beta + R.beta;
-  const double pm = 0.5 * (L.rho + R.rho) / bsum;
+  double rho_m, drho_m, ib, dib, rrs, rbs;
+  const double rsum = L.rho + R.rho, bsum = L.beta + R.beta;
+  two_reciprocals(rsum, bsum, rrs, rbs);
+  ln_mean_dx(L.rho, R.rho, rrs, rho_m, drho_m);
+  inv_ln_mean_dx(L.beta, R.beta, rbs, ib, dib);
+  const double pm = 0.5 * rsum * rbs;
   const double f1 = rho_m * 0.5 * (vnL + vnR);
   const double va[2] = {0.5 * (L.v[0] + R.v[0]), 0.5 * (L.v[1] + R.v[1])};
   const double fm[2] = {f1 * va[0] + pm * n[0], f1 * va[1] + pm * n[1]};
@@ -127,15 +137,15 @@ __device__ __forceinline__ void ec_flux_vjp_left(const NodeState<2>& L, const No
 #pragma unroll
   for (int d = 0; d < 2; ++d) vb[d] += 0.5 * (c[3] * fm[d] + fmb[d] * f1) + vnb * n[d];
   kb += -0.5 * Ab;
-  rb += pmb * 0.5 / bsum + f1b * 0.5 * (vnL + vnR) * drho_m;
-  bb += -pmb * pm / bsum + 0.5 * igm1 * Ab * dib;
+  rb += pmb * 0.5 * rbs + f1b * 0.5 * (vnL + vnR) * drho_m;
+  bb += -pmb * pm * rbs + 0.5 * igm1 * Ab * dib;
 }
 
 // Chain rule from primitive cotangents (rho, v, p) to conserved ones, with
 // v = m / rho and p = (gamma - 1)(E - |m|^2 / (2 rho)).
 __device__ __forceinline__ void prim_to_cons_vjp(const double* u, double gm1, double rb,
-                                                 const double* vb, double pb, double* ub) {
-  const double inv_rho = 1.0 / u[0];
+                                                 const double* vb, double pb, double* ub,
+                                                 double inv_rho) {
   const double v0 = u[1] * inv_rho, v1 = u[2] * inv_rho;
   ub[0] += rb + gm1 * pb * 0.5 * (v0 * v0 + v1 * v1) - (vb[0] * v0 + vb[1] * v1) * inv_rho;
   ub[1] += vb[0] * inv_rho - gm1 * pb * v0;
@@ -178,13 +188,15 @@ __device__ __forceinline__ void llf_vjp(const FaceState<2>& L, const FaceState<2
   const double aO = own_left ? aL : aR;
   if (own_v) vnb += lamb * (vnO >= 0.0 ? 1.0 : -1.0);
   double rb = 0.0;
+  double iaO, iuO;  // 1 / a and 1 / rho of the own side
+  two_reciprocals(aO, O.u[0], iaO, iuO);
   if (own_a) {
     const double ab = lamb * sn;  // a = sqrt(gamma p / rho)
-    pb += ab * gamma / (2.0 * aO * O.u[0]);
-    rb += -ab * aO / (2.0 * O.u[0]);
+    pb += ab * gamma * 0.5 * iaO * iuO;
+    rb += -ab * aO * 0.5 * iuO;
   }
   const double vb[2] = {vnb * n[0], vnb * n[1]};
-  prim_to_cons_vjp(O.u, gamma - 1.0, rb, vb, pb, uo);
+  prim_to_cons_vjp(O.u, gamma - 1.0, rb, vb, pb, uo, iuO);
 #pragma unroll
   for (int q = 0; q < 4; ++q) ub[q] += uo[q];
 }
@@ -369,10 +381,12 @@ __global__ void __launch_bounds__(EPB* N* N) adj_main_kernel(const AdjArgs<N> p)
   const FaceState<2> fo = prepare_face<2>(u, p.gamma);
   {
     // beta = rho / (2 p), kin = |v|^2 / 2
-    const double rbt = rb + bb * 0.5 / fo.p;
-    const double pb = -bb * own.beta / fo.p;
+    double ip, iu;
+    two_reciprocals(fo.p, u[0], ip, iu);
+    const double rbt = rb + bb * 0.5 * ip;
+    const double pb = -bb * own.beta * ip;
     const double vbt[2] = {vb[0] + kb * own.v[0], vb[1] + kb * own.v[1]};
-    prim_to_cons_vjp(u, gm1, rbt, vbt, pb, ub);
+    prim_to_cons_vjp(u, gm1, rbt, vbt, pb, ub, iu);
   }
 
   // -- LLF interface fluxes of the element's faces through this node
@@ -448,9 +462,10 @@ __global__ void __launch_bounds__(EPB* N* N) adj_main_kernel(const AdjArgs<N> p)
     double qv[4];
     ns_gradient_variables(u, p.gamma, qv);
     const double T = qv[3];
-    const double rbq = qb[0] - qb[3] * T / u[0];
+    const double iu = 1.0 / u[0];
+    const double rbq = qb[0] - qb[3] * T * iu;
     const double vbq[2] = {qb[1], qb[2]};
-    prim_to_cons_vjp(u, gm1, rbq, vbq, qb[3] / u[0], ub);
+    prim_to_cons_vjp(u, gm1, rbq, vbq, qb[3] * iu, ub, iu);
   }
 
   // -- epilogue
