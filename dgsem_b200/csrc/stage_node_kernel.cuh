@@ -280,7 +280,10 @@ __device__ __forceinline__ void node_volume_direction(const StageArgs<N>& p, con
           acc[q] += dmb * xbuf[((o - 1) * NV + q) * nth + tid + back * SN];
       }
     }
-    __syncthreads();  // the buffer is reused by the next direction
+    // direction 1 reuses the buffer; after direction 1 (the last one that
+    // exchanges: z lines never do) the block passes another barrier before
+    // anything writes it again
+    if constexpr (DIR == 0) __syncthreads();
   }
 }
 
