@@ -277,8 +277,8 @@ __global__ void __launch_bounds__(EPB* N* N) adj_viscous_kernel(const AdjArgs<N>
     gx[v] = __ldg(p.grad + (((int64_t)e * 4 + v) * 2 + 0) * ND + node);
     gy[v] = __ldg(p.grad + (((int64_t)e * 4 + v) * 2 + 1) * ND + node);
   }
-  const double tau11 = (4.0 * gx[1] - 2.0 * gy[2]) / 3.0;
-  const double tau22 = (4.0 * gy[2] - 2.0 * gx[1]) / 3.0;
+  const double tau11 = (4.0 * gx[1] - 2.0 * gy[2]) * (1.0 / 3.0);
+  const double tau22 = (4.0 * gy[2] - 2.0 * gx[1]) * (1.0 / 3.0);
   const double tau12 = gy[1] + gx[2];
   const double t11b = sx[1] + sx[3] * q[1];
   const double t12b = sx[2] + sx[3] * q[2] + sy[1] + sy[3] * q[1];
@@ -288,10 +288,10 @@ __global__ void __launch_bounds__(EPB* N* N) adj_viscous_kernel(const AdjArgs<N>
   double Gb[4][2];
   Gb[0][0] = 0.0;
   Gb[0][1] = 0.0;
-  Gb[1][0] = (4.0 * t11b - 2.0 * t22b) / 3.0;
+  Gb[1][0] = (4.0 * t11b - 2.0 * t22b) * (1.0 / 3.0);
   Gb[1][1] = t12b;
   Gb[2][0] = t12b;
-  Gb[2][1] = (4.0 * t22b - 2.0 * t11b) / 3.0;
+  Gb[2][1] = (4.0 * t22b - 2.0 * t11b) * (1.0 / 3.0);
   Gb[3][0] = p.kappa * sx[3];
   Gb[3][1] = p.kappa * sy[3];
   const double ij = adj_inv_j<N>(p.tab, ie, je, node);

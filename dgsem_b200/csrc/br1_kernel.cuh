@@ -32,12 +32,14 @@ __device__ __forceinline__ void ns_gradient_variables(const double* u, double ga
 }
 
 // Viscous flux -F_v in direction dim (compressible_navier_stokes2D.hpp:71-106;
-// the solver stores -F_v, parabolic_viscous.hpp:383-387).
+// the solver stores -F_v, parabolic_viscous.hpp:383-387).  The 1/3 of the
+// normal stresses is a multiplication by the rounded constant 1/3 (a
+// division by 3 costs a full division sequence per stress).
 __device__ __forceinline__ void ns_neg_viscous_flux(const double* q, const double* gx,
                                                     const double* gy, double mu,
                                                     double kappa, int dim, double* f) {
-  const double tau11 = (4.0 * gx[1] - 2.0 * gy[2]) / 3.0;
-  const double tau22 = (4.0 * gy[2] - 2.0 * gx[1]) / 3.0;
+  const double tau11 = (4.0 * gx[1] - 2.0 * gy[2]) * (1.0 / 3.0);
+  const double tau22 = (4.0 * gy[2] - 2.0 * gx[1]) * (1.0 / 3.0);
   const double tau12 = gy[1] + gx[2];
   f[0] = -0.0;
   if (dim == 0) {
@@ -73,9 +75,9 @@ __device__ __forceinline__ void ns_neg_viscous_flux_3d(const double* q, const do
   const double dv1dx = g[0][0], dv2dx = g[0][1], dv3dx = g[0][2];
   const double dv1dy = g[1][0], dv2dy = g[1][1], dv3dy = g[1][2];
   const double dv1dz = g[2][0], dv2dz = g[2][1], dv3dz = g[2][2];
-  const double tau11 = (4.0 * dv1dx - 2.0 * (dv2dy + dv3dz)) / 3.0;
-  const double tau22 = (4.0 * dv2dy - 2.0 * (dv1dx + dv3dz)) / 3.0;
-  const double tau33 = (4.0 * dv3dz - 2.0 * (dv1dx + dv2dy)) / 3.0;
+  const double tau11 = (4.0 * dv1dx - 2.0 * (dv2dy + dv3dz)) * (1.0 / 3.0);
+  const double tau22 = (4.0 * dv2dy - 2.0 * (dv1dx + dv3dz)) * (1.0 / 3.0);
+  const double tau33 = (4.0 * dv3dz - 2.0 * (dv1dx + dv2dy)) * (1.0 / 3.0);
   const double tau12 = dv1dy + dv2dx;
   const double tau13 = dv1dz + dv3dx;
   const double tau23 = dv2dz + dv3dy;
