@@ -1,6 +1,6 @@
 // Minimal sm_100a helpers for one-dimensional bulk (TMA) copies from global
 // to shared memory completed on an mbarrier.  Plain copies into the issuing
-// CTA's own shared memory; no cluster multicast.
+// CTA's own shared memory, from this GPU's own global memory only.
 #pragma once
 
 #include <cuda_runtime.h>
